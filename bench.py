@@ -1,0 +1,289 @@
+#!/usr/bin/env python3
+"""Throughput of the one-table suffix-table engine: prime-residues/s at n=16384, M=32768, d=3.
+
+One step = one batch of B primes through the hot path: per-prime tables, the n-1 suffix-table
+steps (two 1/t convolutions each), the nbad(n, M) query and the Horner finish, for every prime.
+A prime-residue is one (d, prime) table built to n plus the residue of its query.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N > 1) each rank takes its own disjoint prime range (weak scaling, no collective
+on the data path); the time is the max over ranks.  `--impl reference` times the reference's own
+CPU build (oracle/_ref/cuckoo_fast_ifma, or _cpu without AVX-512 IFMA) in one process per host
+core on disjoint primes, the reference's documented way to split a run.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cuckoo-failure_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "prime-residues/s, n=16384 d=3 NTT suffix build; served-query p50/p99 latency"
+UNIT = "prime-residues/s"
+K_OPS_PER_MM = 20  # INT32 multiply ops per 64-bit modular multiplication (fixed accounting model)
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def algorithmic_mm(n):
+    """Modular multiplications per prime-residue (one table to n plus one query): two convolutions
+    per step of L (lg + 1) each, the stage pre/post products (about 6.5 n^2) and the query (1.5 n^2)."""
+    L = 16
+    while L < n:
+        L *= 2
+    lg = L.bit_length() - 1
+    return 2 * (n - 1) * L * (lg + 1) + 8 * n * n
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_binary():
+    ifma = os.path.join(REF_DIR, "cuckoo_fast_ifma")
+    has_ifma = "avx512ifma" in open("/proc/cpuinfo").read()
+    if has_ifma and os.path.exists(ifma):
+        return ifma, "AVX-512 IFMA build (make fast-ifma)"
+    return os.path.join(REF_DIR, "cuckoo_fast_cpu"), "scalar host build (make fast)"
+
+
+def run_reference_wave(binary, n, M, d, first, procs):
+    """One process per core, each one prime of the fixed list (disjoint FIRST COUNT ranges).
+    Returns (seconds, output lines)."""
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(f"{n} {M}\n")
+        qpath = f.name
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen([binary, str(d), qpath, str(first + k), "1"], stdout=subprocess.PIPE,
+                           stderr=subprocess.DEVNULL, text=True) for k in range(procs)]
+    outs = [p.communicate()[0] for p in ps]
+    dt = time.perf_counter() - t0
+    os.unlink(qpath)
+    if any(p.returncode for p in ps):
+        raise RuntimeError("reference binary failed")
+    return dt, [ln for o in outs for ln in o.splitlines()]
+
+
+def cpu_baseline(n, M, d):
+    binary, kind = reference_binary()
+    P = host_cores()
+    dt, lines = run_reference_wave(binary, n, M, d, 0, P)
+    return {"value": P / dt, "unit": UNIT, "cores": P, "kind": "reference",
+            "sample": f"{P} processes x 1 prime (primes 0..{P - 1}) of n={n}, M={M}, d={d} with the reference's "
+                      f"{kind}, {dt:.1f} s wall"}
+
+
+def golden_check(n, M, d):
+    """Known residues of the reference host build for primes 0 and 1 (tests/golden)."""
+    path = os.path.join(ROOT, "tests", "golden", f"fast_n{n}_d{d}.txt")
+    if not os.path.exists(path):
+        return {}
+    out = {}
+    with open(path) as f:
+        for ln in f:
+            t = ln.split()
+            if len(t) == 5 and not ln.startswith("#") and int(t[2]) == n and int(t[3]) == M:
+                out[int(t[0])] = int(t[4])
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=16384)
+    ap.add_argument("--M", type=int, default=32768)
+    ap.add_argument("--d", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=0, help="primes per step per GPU (default: one wave)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic-bytes", type=float, default=None,
+                    help="DRAM bytes per launch of the main kernel from an ncu capture (roofline.traffic)")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+    n, M, d = a.n, a.M, a.d
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    workload = f"one-table suffix build + nbad query, n={n}, M={M}, d={d}, 50-bit primes of the fixed list"
+
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        binary, kind = reference_binary()
+        if not os.path.exists(binary):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (run make -f oracle/Makefile.ref)"}))
+            return 0
+        P = host_cores()
+        times = []
+        for s in range(a.warmup + a.steps):
+            dt, _ = run_reference_wave(binary, n, M, d, s * P, P)
+            if s >= a.warmup:
+                times.append(dt)
+        tot = sum(times)
+        v = P * a.steps / tot
+        print(json.dumps({
+            "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": workload, "batch_primes_per_step": P, "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": P, "kind": "reference",
+                             "sample": f"each step {P} processes x 1 prime with the reference's {kind}"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import cuckoo_b200 as cb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    eng = cb.Engine(local)
+    queries = [(n, M)]
+    J = 1
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    B = a.batch or min(eng.max_batch(n, M, J), sms)
+    primes = cb.prime_range(rank * B, B)
+    stream = torch.cuda.current_stream()
+    d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
+    d_out = torch.empty(B * J, dtype=torch.int64, device="cuda")
+
+    def step():
+        eng.residues_async(d_primes.data_ptr(), B, n, d, queries, d_out.data_ptr(), stream.cuda_stream)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    # self-check against the reference's residues for the primes it covers
+    got = d_out.cpu().numpy().view(np.uint64)
+    for i, r in golden_check(n, M, d).items():
+        if rank == 0 and i < B:
+            assert int(got[i]) == r, f"residue mismatch at prime {i}: {int(got[i])} != {r}"
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    launches = 0
+    barrier()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+            launches += eng.last_launches()
+        e1.record(stream)
+        barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * B * a.steps / (ms * 1e-3)
+
+    # end to end through the public API with host buffers (copies inside the timed region)
+    host_primes = np.array(primes, dtype=np.uint64)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        res = eng.residues(host_primes, n, d, queries)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": world * B * a.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * B + 8 * J + 4,
+           "d2h_bytes_per_step": 8 * B * J + 4}
+    assert np.array_equal(res.reshape(-1), got[:B * J]), "e2e residues differ from the device-timed run"
+
+    probe = ctypes.CDLL(os.path.join(PKG, "lib", "libcuckoo_b200_probe.so"))
+    probe.cfp_imad_ops_per_s.restype = ctypes.c_double
+    probe.cfp_imad_ops_per_s.argtypes = [ctypes.c_int, ctypes.c_int]
+    peak = probe.cfp_imad_ops_per_s(local, 5) / 1e12
+    # the timed stream holds only this engine's launches, back to back: per-GPU algorithmic rate
+    achieved = B * a.steps * algorithmic_mm(n) * K_OPS_PER_MM / (ms * 1e-3) / 1e12
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(reference_binary()[0]):
+        cpu = cpu_baseline(n, M, d)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64", "data": "synthetic",
+            "config": {"workload": workload, "batch_primes_per_step": B, "queries_per_prime": J,
+                       "l2": "inputs larger than L2 (per-prime tables total far above 126 MB)"},
+            "roofline": {"bound": "int32", "achieved": achieved, "peak": peak, "unit": "Top/s (INT32 IMAD)",
+                         "frac": achieved / peak if peak else None, "traffic": a.traffic_bytes,
+                         "model": f"{K_OPS_PER_MM} INT32 multiply ops per modular multiplication, "
+                                  f"{algorithmic_mm(n):.3e} multiplications per prime-residue; peak measured live"},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,300 @@
+// CUDA implementation of the C ABI in include/cuckoo_b200.h: the persistent per-prime kernel
+// (one CTA per prime, all steps in one launch) and the host-side batching around it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cuckoo_b200.h"
+#include "host_common.hpp"
+#include "kernel_lg.cuh"
+
+using namespace cfb;
+
+cfb::KInfo cf_kinfo_lg4();
+cfb::KInfo cf_kinfo_lg5();
+cfb::KInfo cf_kinfo_lg6();
+cfb::KInfo cf_kinfo_lg7();
+cfb::KInfo cf_kinfo_lg8();
+cfb::KInfo cf_kinfo_lg9();
+cfb::KInfo cf_kinfo_lg10();
+cfb::KInfo cf_kinfo_lg11();
+cfb::KInfo cf_kinfo_lg12();
+cfb::KInfo cf_kinfo_lg13();
+cfb::KInfo cf_kinfo_lg14();
+static KInfo kernel_for(int lg) {
+    switch (lg) {
+        case 4: return cf_kinfo_lg4();
+        case 5: return cf_kinfo_lg5();
+        case 6: return cf_kinfo_lg6();
+        case 7: return cf_kinfo_lg7();
+        case 8: return cf_kinfo_lg8();
+        case 9: return cf_kinfo_lg9();
+        case 10: return cf_kinfo_lg10();
+        case 11: return cf_kinfo_lg11();
+        case 12: return cf_kinfo_lg12();
+        case 13: return cf_kinfo_lg13();
+        case 14: return cf_kinfo_lg14();
+        default: return KInfo{nullptr, 0, 0};
+    }
+}
+static constexpr int MAX_LG = 14;
+
+// ------------------------------------------------------------------------------------------
+// Engine
+// ------------------------------------------------------------------------------------------
+struct cf_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    u64* ws = nullptr;  // workspace
+    size_t ws_bytes = 0;
+    int* d_err = nullptr;
+    int* d_q = nullptr;  // [2][qcap] query n and M
+    int qcap = 0;
+    u64* d_primes = nullptr;  // staging for cf_residues
+    u64* d_out = nullptr;
+    size_t io_cap = 0;  // primes capacity of d_primes; d_out has io_cap * jcap
+    int jcap = 0;
+    long launches = 0;
+    std::string err;
+};
+
+static int fail(cf_engine* e, int code, const std::string& msg) {
+    if (e) e->err = msg;
+    return code;
+}
+static int cuda_fail(cf_engine* e, cudaError_t c, const char* what) {
+    return fail(e, CF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(c));
+}
+#define CF_CUDA(call, what)                              \
+    do {                                                 \
+        cudaError_t c_ = (call);                         \
+        if (c_ != cudaSuccess) return cuda_fail(e, c_, what); \
+    } while (0)
+
+struct Plan {
+    int lg, F, d0;
+    size_t ws_words;
+};
+
+static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const int* qM, int J, Plan& pl) {
+    if (nmax < 1 || d < 1 || (model != CF_MODEL_SUBSET && model != CF_MODEL_REPLACEMENT) || J < 0)
+        return fail(e, CF_ERR_ARG, "bad nmax, d, model or J");
+    if (J > 0 && (!qn || !qM)) return fail(e, CF_ERR_ARG, "null query arrays");
+    int F = nmax;
+    for (int j = 0; j < J; ++j) {
+        if (qn[j] < 1 || qn[j] > nmax || qM[j] <= qn[j]) return fail(e, CF_ERR_ARG, "query needs 1 <= n <= nmax and M > n");
+        if (model == CF_MODEL_SUBSET && d > qM[j]) return fail(e, CF_ERR_ARG, "subset model needs d <= M");
+        F = std::max(F, qM[j]);
+    }
+    if (model == CF_MODEL_SUBSET && d > F) F = d;  // ifact[d] is read for g(v)
+    const u64 L = cfh::transform_length((u64)nmax);
+    int lg = 0;
+    while ((1ull << lg) < L) ++lg;
+    if (lg > MAX_LG) return fail(e, CF_ERR_UNSUPPORTED, "transform length above 2^14 (nmax > 16384) is not supported by this build");
+    pl.lg = lg;
+    pl.F = F;
+    pl.d0 = model == CF_MODEL_SUBSET ? d : 1;
+    pl.ws_words = make_layout(nmax, F, (int)L, J).total;
+    return CF_OK;
+}
+
+static int check_primes(cf_engine* e, const u64* primes, int B, const Plan& pl) {
+    const u64 L = 1ull << pl.lg;
+    for (int b = 0; b < B; ++b) {
+        const u64 p = primes[b];
+        if (p < 3 || (p & 1) == 0 || p >= (1ull << 50) || p <= (u64)pl.F || (p - 1) % L != 0 || !cfh::is_prime(p))
+            return fail(e, CF_ERR_ARG, "prime " + std::to_string(p) + " is not an odd prime < 2^50 above max(n, M) with L | p-1");
+    }
+    return CF_OK;
+}
+
+static int ensure_ws(cf_engine* e, size_t bytes) {
+    if (e->ws_bytes >= bytes) return CF_OK;
+    if (e->ws) cudaFree(e->ws);
+    e->ws = nullptr;
+    e->ws_bytes = 0;
+    CF_CUDA(cudaMalloc(&e->ws, bytes), "workspace allocation");
+    e->ws_bytes = bytes;
+    return CF_OK;
+}
+static int ensure_queries(cf_engine* e, const int* qn, const int* qM, int J, cudaStream_t s) {
+    if (J > e->qcap) {
+        if (e->d_q) cudaFree(e->d_q);
+        e->d_q = nullptr;
+        CF_CUDA(cudaMalloc(&e->d_q, sizeof(int) * 2 * (size_t)J), "query allocation");
+        e->qcap = J;
+    }
+    if (J) {
+        CF_CUDA(cudaMemcpyAsync(e->d_q, qn, sizeof(int) * J, cudaMemcpyHostToDevice, s), "query upload");
+        CF_CUDA(cudaMemcpyAsync(e->d_q + e->qcap, qM, sizeof(int) * J, cudaMemcpyHostToDevice, s), "query upload");
+    }
+    return CF_OK;
+}
+
+static long fit_batch(size_t per_prime) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
+    const size_t reserve = (size_t)1 << 30;  // leave 1 GiB for the context, staging and other users
+    if (fr <= reserve) return 0;
+    return (long)((fr - reserve) / per_prime);
+}
+
+static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int d, int model, int J, const Plan& pl,
+                        u64* d_out, cudaStream_t s) {
+    const KInfo ki = kernel_for(pl.lg);
+    if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
+    CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ki.smem),
+            "shared memory attribute");
+    const size_t per_prime = pl.ws_words * 8;
+    // chunk: as many primes as the workspace (grown once) holds
+    long cap = (long)(e->ws_bytes / per_prime);
+    if (cap < B) {
+        long fitb = fit_batch(per_prime) + cap;  // what is free plus what is already held
+        if (fitb < 1) return fail(e, CF_ERR_NOMEM, "not enough device memory for one prime");
+        const long want = std::min<long>(B, fitb);
+        int rc = ensure_ws(e, (size_t)want * per_prime);
+        if (rc) return rc;
+        cap = want;
+    }
+    CF_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(int), s), "error reset");
+    for (int at = 0; at < B; at += (int)cap) {
+        const int nb = (int)std::min<long>(cap, B - at);
+        KParams kp;
+        kp.primes = d_primes + at;
+        kp.B = nb;
+        kp.n = nmax;
+        kp.F = pl.F;
+        kp.d = d;
+        kp.d0 = pl.d0;
+        kp.model = model;
+        kp.J = J;
+        kp.qn = e->d_q;
+        kp.qM = e->d_q + e->qcap;
+        kp.ws = e->ws;
+        kp.ws_words = pl.ws_words;
+        kp.out = d_out + (size_t)at * J;
+        kp.err = e->d_err;
+        ki.fn<<<nb, ki.threads, ki.smem, s>>>(kp);
+        CF_CUDA(cudaGetLastError(), "kernel launch");
+        ++e->launches;
+    }
+    return CF_OK;
+}
+
+extern "C" {
+
+long cf_prime_range(long first, long count, uint64_t* out) {
+    if (first < 0 || count < 0 || (count > 0 && !out)) return 0;
+    const std::vector<u64> v = cfh::prime_range(first, count);
+    std::copy(v.begin(), v.end(), out);
+    return (long)v.size();
+}
+long cf_need(int n, int M, int d, int model) { return cfh::need(n, M, d, model); }
+uint64_t cf_transform_length(uint64_t nmax) { return cfh::transform_length(nmax); }
+
+int cf_engine_create(int device, cf_engine** out) {
+    if (!out) return CF_ERR_ARG;
+    *out = nullptr;
+    cf_engine* e = new cf_engine();
+    e->device = device;
+    cudaError_t c = cudaSetDevice(device);
+    if (c == cudaSuccess) c = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (c == cudaSuccess) c = cudaMalloc(&e->d_err, sizeof(int));
+    if (c != cudaSuccess) {
+        delete e;
+        return CF_ERR_CUDA;
+    }
+    *out = e;
+    return CF_OK;
+}
+
+void cf_engine_destroy(cf_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    cudaFree(e->ws);
+    cudaFree(e->d_err);
+    cudaFree(e->d_q);
+    cudaFree(e->d_primes);
+    cudaFree(e->d_out);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+const char* cf_engine_last_error(const cf_engine* e) { return e ? e->err.c_str() : "no engine"; }
+long cf_last_launches(const cf_engine* e) { return e ? e->launches : 0; }
+
+uint64_t cf_workspace_bytes(int nmax, int Mmax, int J) {
+    if (nmax < 1 || J < 0) return 0;
+    const int F = std::max(nmax, Mmax);
+    return 8 * make_layout(nmax, F, (int)cfh::transform_length((u64)nmax), J).total;
+}
+
+long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J) {
+    if (!e) return 0;
+    cudaSetDevice(e->device);
+    const uint64_t per = cf_workspace_bytes(nmax, Mmax, J);
+    if (!per) return 0;
+    return fit_batch(per) + (long)(e->ws_bytes / per);
+}
+
+int cf_residues_async(cf_engine* e, const uint64_t* d_primes, int B, int nmax, int d, int model, const int* qn,
+                      const int* qM, int J, uint64_t* d_residues, void* stream) {
+    if (!e) return CF_ERR_ARG;
+    e->err.clear();
+    e->launches = 0;
+    if (B < 0 || (B > 0 && (!d_primes || (J > 0 && !d_residues)))) return fail(e, CF_ERR_ARG, "bad batch buffers");
+    Plan pl;
+    int rc = plan(e, nmax, d, model, qn, qM, J, pl);
+    if (rc) return rc;
+    if (B == 0) return CF_OK;
+    CF_CUDA(cudaSetDevice(e->device), "set device");
+    cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+    rc = ensure_queries(e, qn, qM, J, s);
+    if (rc) return rc;
+    return launch_batch(e, d_primes, B, nmax, d, model, J, pl, d_residues, s);
+}
+
+int cf_residues(cf_engine* e, const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM,
+                int J, uint64_t* residues) {
+    if (!e) return CF_ERR_ARG;
+    e->err.clear();
+    e->launches = 0;
+    if (B < 0 || (B > 0 && (!primes || (J > 0 && !residues)))) return fail(e, CF_ERR_ARG, "bad batch buffers");
+    Plan pl;
+    int rc = plan(e, nmax, d, model, qn, qM, J, pl);
+    if (rc) return rc;
+    rc = check_primes(e, primes, B, pl);
+    if (rc) return rc;
+    if (B == 0) return CF_OK;
+    CF_CUDA(cudaSetDevice(e->device), "set device");
+    cudaStream_t s = e->stream;
+    if ((size_t)B > e->io_cap || J > e->jcap) {
+        cudaFree(e->d_primes);
+        cudaFree(e->d_out);
+        e->d_primes = nullptr;
+        e->d_out = nullptr;
+        e->io_cap = 0;
+        CF_CUDA(cudaMalloc(&e->d_primes, 8 * (size_t)B), "prime buffer");
+        CF_CUDA(cudaMalloc(&e->d_out, 8 * (size_t)B * std::max(J, 1)), "residue buffer");
+        e->io_cap = (size_t)B;
+        e->jcap = std::max(J, 1);
+    }
+    CF_CUDA(cudaMemcpyAsync(e->d_primes, primes, 8 * (size_t)B, cudaMemcpyHostToDevice, s), "prime upload");
+    rc = ensure_queries(e, qn, qM, J, s);
+    if (rc) return rc;
+    rc = launch_batch(e, e->d_primes, B, nmax, d, model, J, pl, e->d_out, s);
+    if (rc) return rc;
+    int herr = 0;
+    if (J) CF_CUDA(cudaMemcpyAsync(residues, e->d_out, 8 * (size_t)B * J, cudaMemcpyDeviceToHost, s), "residue download");
+    CF_CUDA(cudaMemcpyAsync(&herr, e->d_err, sizeof(int), cudaMemcpyDeviceToHost, s), "error download");
+    CF_CUDA(cudaStreamSynchronize(s), "batch");
+    if (herr) return fail(e, CF_ERR_DEVICE, "device check failed (code " + std::to_string(herr) + ")");
+    return CF_OK;
+}
+
+}  // extern "C"

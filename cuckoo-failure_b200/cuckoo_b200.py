@@ -1,0 +1,151 @@
+"""Python binding of the B200 engine's C ABI (include/cuckoo_b200.h) through ctypes.
+
+The reference (zcy05331/Cuckoo-Failure) exposes this path as the `cuckoo_fast` CLI
+(fast/cuckoo_fast.cu:648-904); this module offers the same operations to Python callers:
+
+    prime_range(first, count)          fixed prime list           (fast/cuckoo_fast.cu:403-432)
+    need(n, M, d, model)               primes a query needs      (fast/cuckoo_fast.cu:452-459)
+    transform_length(nmax)             NTT length                (fast/cuckoo_fast.cu:460-472)
+    Engine(device).residues(...)       one batch of primes       (fast/cuckoo_fast.cu:787-901)
+
+There is no CPU fallback: importing works without a GPU (for the host helpers), but the engine
+raises if the CUDA library is missing or no device is present.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libcuckoo_b200.so")
+CLI_PATH = os.path.join(PKG, "bin", "cuckoo_fast_b200")
+
+MODEL_SUBSET = 0
+MODEL_REPLACEMENT = 1
+
+CF_OK, CF_ERR_ARG, CF_ERR_CUDA, CF_ERR_NOMEM, CF_ERR_UNSUPPORTED, CF_ERR_DEVICE = 0, -1, -2, -3, -4, -5
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_intp = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cuckoo_b200 error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load libcuckoo_b200.so (built by cuckoo-failure_b200/build.py); raise if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python cuckoo-failure_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.cf_prime_range.argtypes = [ctypes.c_long, ctypes.c_long, _u64p]
+        L.cf_prime_range.restype = ctypes.c_long
+        L.cf_need.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.cf_need.restype = ctypes.c_long
+        L.cf_transform_length.argtypes = [ctypes.c_uint64]
+        L.cf_transform_length.restype = ctypes.c_uint64
+        L.cf_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.cf_engine_create.restype = ctypes.c_int
+        L.cf_engine_destroy.argtypes = [ctypes.c_void_p]
+        L.cf_engine_destroy.restype = None
+        L.cf_engine_last_error.argtypes = [ctypes.c_void_p]
+        L.cf_engine_last_error.restype = ctypes.c_char_p
+        L.cf_residues.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  _intp, _intp, ctypes.c_int, _u64p]
+        L.cf_residues.restype = ctypes.c_int
+        L.cf_residues_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, _intp, _intp, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.cf_residues_async.restype = ctypes.c_int
+        L.cf_workspace_bytes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.cf_workspace_bytes.restype = ctypes.c_uint64
+        L.cf_max_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.cf_max_batch.restype = ctypes.c_long
+        L.cf_last_launches.argtypes = [ctypes.c_void_p]
+        L.cf_last_launches.restype = ctypes.c_long
+        _lib = L
+    return _lib
+
+
+def prime_range(first, count):
+    out = np.zeros(max(count, 0), dtype=np.uint64)
+    got = lib().cf_prime_range(first, count, out.ctypes.data_as(_u64p))
+    return [int(x) for x in out[:got]]
+
+
+def need(n, M, d, model=MODEL_SUBSET):
+    return int(lib().cf_need(n, M, d, model))
+
+
+def transform_length(nmax):
+    return int(lib().cf_transform_length(nmax))
+
+
+def workspace_bytes(nmax, Mmax, J):
+    return int(lib().cf_workspace_bytes(nmax, Mmax, J))
+
+
+def _queries(queries):
+    qn = np.ascontiguousarray([q[0] for q in queries], dtype=np.int32)
+    qM = np.ascontiguousarray([q[1] for q in queries], dtype=np.int32)
+    return qn, qM
+
+
+class Engine:
+    """One CUDA device.  residues() runs one batch of primes through the persistent kernel."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        rc = lib().cf_engine_create(device, ctypes.byref(h))
+        if rc != CF_OK:
+            raise EngineError(rc, f"cannot open CUDA device {device}")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().cf_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != CF_OK:
+            raise EngineError(rc, lib().cf_engine_last_error(self._h).decode())
+
+    def residues(self, primes, nmax, d, queries, model=MODEL_SUBSET):
+        """N_bad(n_j, M_j) mod p for every prime (rows) and query (columns), as a uint64 array."""
+        p = np.ascontiguousarray(primes, dtype=np.uint64)
+        qn, qM = _queries(queries)
+        out = np.zeros((len(p), len(qn)), dtype=np.uint64)
+        rc = lib().cf_residues(self._h, p.ctypes.data_as(_u64p), len(p), nmax, d, model, qn.ctypes.data_as(_intp),
+                               qM.ctypes.data_as(_intp), len(qn), out.ctypes.data_as(_u64p))
+        self._check(rc)
+        return out
+
+    def residues_async(self, d_primes_ptr, B, nmax, d, queries, d_out_ptr, stream_ptr=None, model=MODEL_SUBSET):
+        """Device-pointer variant (e.g. torch tensors' data_ptr()); enqueued on stream_ptr."""
+        qn, qM = _queries(queries)
+        rc = lib().cf_residues_async(self._h, ctypes.c_void_p(d_primes_ptr), B, nmax, d, model,
+                                     qn.ctypes.data_as(_intp), qM.ctypes.data_as(_intp), len(qn),
+                                     ctypes.c_void_p(d_out_ptr), ctypes.c_void_p(stream_ptr or 0))
+        self._check(rc)
+
+    def max_batch(self, nmax, Mmax, J):
+        return int(lib().cf_max_batch(self._h, nmax, Mmax, J))
+
+    def last_launches(self):
+        return int(lib().cf_last_launches(self._h))

@@ -1,0 +1,84 @@
+/* C ABI of the B200 engine for the one-table suffix-table path of zcy05331/Cuckoo-Failure.
+ *
+ * The reference has no FFI: its host driver (fast/cuckoo_fast.cu main) calls a compile-time
+ * execution back end (launch / convolve / dev_alloc / to_dev / from_dev, :325-386, :623-646) and
+ * launches k_query directly (:867-876).  These entry points replace that seam, one call per batch
+ * of primes: everything from the per-prime tables to the residues runs on the GPU.
+ *
+ * Conventions: every function returns an int status (CF_OK = 0, negative on error) and never
+ * exits the process (the reference's cuda_check calls exit(1), :329-334).  The caller owns host
+ * buffers, the engine owns device workspace.  Calls on one engine must not overlap.
+ * Residues are canonical (0 <= r < p), exactly what the reference prints as its fifth column.
+ */
+#ifndef CUCKOO_B200_H
+#define CUCKOO_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cf_status {
+    CF_OK = 0,
+    CF_ERR_ARG = -1,         /* invalid argument (sizes, prime not NTT-friendly, query out of range) */
+    CF_ERR_CUDA = -2,        /* CUDA runtime error (message in cf_engine_last_error) */
+    CF_ERR_NOMEM = -3,       /* not enough device memory for even one prime */
+    CF_ERR_UNSUPPORTED = -4, /* transform length beyond what this build handles */
+    CF_ERR_DEVICE = -5       /* a device-side check failed (e.g. no root of unity of order L) */
+};
+
+/* Sampling models (include/cuckoo/single_table.hpp:16-23). */
+enum cf_model { CF_MODEL_SUBSET = 0, CF_MODEL_REPLACEMENT = 1 };
+
+typedef struct cf_engine cf_engine;
+
+/* ---- host helpers with the reference's exact semantics ---- */
+
+/* Primes number first .. first+count-1 of the fixed list (p = c 2^20 + 1 < 2^50, prime, largest
+ * first).  Replaces prime_range, fast/cuckoo_fast.cu:403-432.  Returns the number written. */
+long cf_prime_range(long first, long count, uint64_t* out);
+
+/* Number of 50-bit primes query (n, M) needs: ceil((n log2 Q + 3) / 49) + 1 in long double.
+ * Replaces need / log2_Q, fast/cuckoo_fast.cu:452-459 (CF_MODEL_REPLACEMENT: log2 Q = d log2 M). */
+long cf_need(int n, int M, int d, int model);
+
+/* max(16, next_pow2(nmax)).  Replaces transform_length, fast/cuckoo_fast.cu:460-472. */
+uint64_t cf_transform_length(uint64_t nmax);
+
+/* ---- engine ---- */
+
+/* Bind a CUDA device and create the engine's stream.  Replaces the CUDA back end's implicit
+ * device setup and the up-front dev_alloc calls, fast/cuckoo_fast.cu:345-358, :759-780. */
+int cf_engine_create(int device, cf_engine** out);
+void cf_engine_destroy(cf_engine* e);
+/* Text of the last error on this engine ("" if none).  Valid until the next call. */
+const char* cf_engine_last_error(const cf_engine* e);
+
+/* One batch: for every prime b, build the suffix table V up to nmax for (d, model) and evaluate
+ * the J queries (qn[j], qM[j]); residues[b*J + j] = N_bad(qn[j], qM[j]) mod primes[b].
+ * Replaces the body of the batch loop, fast/cuckoo_fast.cu:787-901: per-prime tables (:797-839),
+ * the step loop (:841-855), k_query (:867-876) and the Horner finish (:877-890).
+ * Requirements: 1 <= qn[j] <= nmax, qM[j] > qn[j], d <= qM[j] for the subset model, every prime
+ * odd, < 2^50, > max(nmax, qM), with transform_length(nmax) dividing p - 1.
+ * Host buffers; returns when the residues are in `residues`. */
+int cf_residues(cf_engine* e, const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM,
+                int J, uint64_t* residues);
+
+/* Same computation with the primes and residues in device memory, enqueued on `stream`
+ * (a cudaStream_t; NULL selects the engine's own stream); returns without waiting. */
+int cf_residues_async(cf_engine* e, const uint64_t* d_primes, int B, int nmax, int d, int model, const int* qn,
+                      const int* qM, int J, uint64_t* d_residues, void* stream);
+
+/* Device workspace per prime in bytes for a table of nmax with J queries up to Mmax. */
+uint64_t cf_workspace_bytes(int nmax, int Mmax, int J);
+
+/* Largest number of primes one launch can hold in the device's free memory (0 if none). */
+long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J);
+
+/* Kernel launches issued by the last cf_residues / cf_residues_async call. */
+long cf_last_launches(const cf_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,95 @@
+// Test harness (not product code): runs the engine's per-prime phase code from
+// cuckoo-failure_b200/csrc/suffix_engine.cuh on the CPU, one emulated thread after another between
+// barriers, so the index logic of the CUDA kernel can be checked against the oracle without a GPU.
+// It is never linked into the product library and is not a fallback for it.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../cuckoo-failure_b200/csrc/host_common.hpp"
+#include "../../cuckoo-failure_b200/csrc/suffix_engine.cuh"
+
+using namespace cfb;
+
+template <class G>
+struct HostExec {
+    std::vector<Regs<G>> regs;
+    HostExec() : regs(G::T) {}
+    template <class F>
+    void each(F&& f) {
+        for (int t = 0; t < G::T; ++t) f(t, regs[t]);
+    }
+    template <class F>
+    void single(F&& f) {
+        f();
+    }
+    void sync() {}
+    void set_error(int* err, int code) {
+        if (*err == 0) *err = code;
+    }
+    void reduce_mod(u64* red, int T, u64 P) {
+        u64 s = 0;
+        for (int t = 0; t < T; ++t) s = madd(s, red[t], P);
+        red[T] = s;
+    }
+};
+
+template <int LG>
+struct RFor {
+    static constexpr int R = LG >= 10 ? 5 : (LG >= 6 ? LG - 5 : 1);
+};
+
+template <int LG>
+static int run_lg(const KParams& kp) {
+    typedef Geo<LG, RFor<LG>::R> G;
+    std::vector<u64> smem(Smem<G>::WORDS);
+    for (int b = 0; b < kp.B; ++b) {
+        HostExec<G> ex;
+        PrimeRun<G, HostExec<G>> pr(ex, kp, b, smem.data());
+        pr.run();
+    }
+    return 0;
+}
+
+extern "C" int emu_residues(const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM, int J,
+                            uint64_t* out) {
+    int F = nmax;
+    for (int j = 0; j < J; ++j) F = qM[j] > F ? qM[j] : F;
+    if (model == MODEL_SUBSET && d > F) F = d;
+    const int L = (int)cfh::transform_length((uint64_t)nmax);
+    int lg = 0;
+    while ((1 << lg) < L) ++lg;
+    const Layout lo = make_layout(nmax, F, L, J);
+    std::vector<u64> ws(lo.total * (size_t)B);
+    int err = 0;
+    KParams kp;
+    kp.primes = primes;
+    kp.B = B;
+    kp.n = nmax;
+    kp.F = F;
+    kp.d = d;
+    kp.d0 = model == MODEL_SUBSET ? d : 1;
+    kp.model = model;
+    kp.J = J;
+    kp.qn = qn;
+    kp.qM = qM;
+    kp.ws = ws.data();
+    kp.ws_words = lo.total;
+    kp.out = out;
+    kp.err = &err;
+    switch (lg) {
+        case 4: run_lg<4>(kp); break;
+        case 5: run_lg<5>(kp); break;
+        case 6: run_lg<6>(kp); break;
+        case 7: run_lg<7>(kp); break;
+        case 8: run_lg<8>(kp); break;
+        case 9: run_lg<9>(kp); break;
+        case 10: run_lg<10>(kp); break;
+        case 11: run_lg<11>(kp); break;
+        case 12: run_lg<12>(kp); break;
+        case 13: run_lg<13>(kp); break;
+        case 14: run_lg<14>(kp); break;
+        default: return -4;
+    }
+    return err ? -5 : 0;
+}

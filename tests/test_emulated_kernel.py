@@ -1,0 +1,45 @@
+"""The engine's per-prime phase code (the same source the CUDA kernel compiles) executed on the
+CPU thread by thread, against the oracle and the reference's golden residues.  This checks the
+transform passes, the stage index arithmetic and the query/Horner phases without a GPU."""
+import pytest
+
+import helpers as h
+
+P0 = 1125899865948161
+
+
+@pytest.mark.parametrize("model", [0, 1])
+@pytest.mark.parametrize("nmax,d,queries", [
+    (1, 2, [(1, 2)]), (5, 1, [(5, 9)]), (8, 2, [(8, 9), (5, 20)]), (16, 3, [(16, 17), (10, 30)]),
+    (20, 3, [(20, 40)]), (33, 3, [(33, 99)]), (64, 1, [(64, 100)]), (200, 3, [(200, 400), (64, 200)]),
+    (256, 4, [(256, 600), (100, 101)]), (300, 2, [(300, 301), (3, 4)]),
+])
+def test_emulated_kernel_matches_oracle(nmax, d, queries, model):
+    assert h.emu_residues([P0], nmax, d, queries, model)[0] == h.oracle_residues(P0, nmax, d, queries, model)
+
+
+def test_emulated_kernel_r5_geometry():
+    """L = 1024 and 2048: five-level register passes (the geometry of the large transforms)."""
+    ps = h.oracle_primes(0, 2)
+    for nmax, d, qs in ((1000, 3, [(1000, 2000), (999, 1001)]), (1024, 2, [(1024, 3000), (7, 9)])):
+        assert h.emu_residues(ps, nmax, d, qs) == [h.oracle_residues(p, nmax, d, qs) for p in ps]
+
+
+def test_emulated_kernel_golden_small():
+    d, queries, first, count, lines = h.load_fast_golden("fast_small_d3.txt")
+    exp = h.expected_by_prime(lines)
+    items = sorted(exp.items())[:3]
+    primes = [p for (i, p), _ in items]
+    got = h.emu_residues(primes, max(n for n, _ in queries), d, queries)
+    for ((i, p), want), row in zip(items, got):
+        for q, r in zip(queries, row):
+            if q in want:
+                assert r == want[q], (i, q)
+
+
+def test_emulated_kernel_32bit_library_primes():
+    """The engine accepts any NTT-friendly odd prime: the library CLI's 32-bit ones (config 1)."""
+    for rec in h.load_lib_golden():
+        if rec[0] == "mod" and rec[2] >= 20:
+            _, rep, n, M, d, P, r = rec
+            assert h.emu_residues([P], n, d, [(n, M)], rep) == [[r]], rec

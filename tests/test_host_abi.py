@@ -1,0 +1,52 @@
+"""The C ABI library: it loads, exports every symbol include/cuckoo_b200.h declares, and its
+host helpers (prime list, need, transform length) agree with the oracle.  No GPU calls."""
+import ctypes
+import os
+import re
+
+import cuckoo_b200 as cb
+import helpers as h
+
+HEADER = os.path.join(h.ROOT, "include", "cuckoo_b200.h")
+
+
+def declared_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(cf_[a-z_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = cb.lib()
+    names = declared_functions()
+    assert len(names) >= 10
+    for name in names:
+        assert hasattr(L, name), name
+
+
+def test_prime_range_matches_oracle():
+    assert cb.prime_range(0, 50) == h.oracle_primes(0, 50)
+    assert cb.prime_range(1000, 7) == h.oracle_primes(1000, 7)
+    assert cb.prime_range(5, 0) == []
+
+
+def test_need_matches_oracle_long_double():
+    o = h.oracle()
+    for d in (1, 2, 3, 4):
+        for n in (1, 8, 20, 200, 511, 4096, 16384):
+            for M in (n + 1, 2 * n, 3 * n + 7, 4 * n):
+                if d > M:
+                    continue
+                for model in (0, 1):
+                    assert cb.need(n, M, d, model) == o.oc_need(n, M, d, model), (n, M, d, model)
+
+
+def test_transform_length():
+    for n in (1, 15, 16, 17, 200, 256, 257, 16384):
+        assert cb.transform_length(n) == h.oracle().oc_transform_length(n)
+
+
+def test_workspace_bytes_grows_quadratically():
+    a, b = cb.workspace_bytes(4096, 8192, 1), cb.workspace_bytes(8192, 16384, 1)
+    assert 3.5 < b / a < 4.5
+    assert cb.workspace_bytes(16384, 32768, 1) >= 16384 * 16384 * 8  # V and S: n^2 words
