@@ -206,7 +206,7 @@ def main():
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     B = a.batch or min(eng.max_batch(n, M, J), sms)
     primes = cb.prime_range(rank * B, B)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a dedicated stream: the events below are recorded on it
     d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
     d_out = torch.empty(B * J, dtype=torch.int64, device="cuda")
 

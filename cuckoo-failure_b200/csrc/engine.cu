@@ -77,8 +77,14 @@ static int cuda_fail(cf_engine* e, cudaError_t c, const char* what) {
 
 struct Plan {
     int lg, F, d0;
+    Layout lay;
     size_t ws_words;
 };
+// warps per CTA of the kernel for transform length 2^lg (query partial sums are kept per warp)
+static int warps_for(int lg) {
+    const KInfo ki = kernel_for(lg);
+    return ki.threads >= 32 ? ki.threads / 32 : 1;
+}
 
 static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const int* qM, int J, Plan& pl) {
     if (nmax < 1 || d < 1 || (model != CF_MODEL_SUBSET && model != CF_MODEL_REPLACEMENT) || J < 0)
@@ -98,7 +104,8 @@ static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const i
     pl.lg = lg;
     pl.F = F;
     pl.d0 = model == CF_MODEL_SUBSET ? d : 1;
-    pl.ws_words = make_layout(nmax, F, (int)L, J).total;
+    pl.lay = make_layout(nmax, F, (int)L, J, warps_for(lg));
+    pl.ws_words = pl.lay.total;
     return CF_OK;
 }
 
@@ -176,6 +183,7 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
         kp.qM = e->d_q + e->qcap;
         kp.ws = e->ws;
         kp.ws_words = pl.ws_words;
+        kp.lay = pl.lay;
         kp.out = d_out + (size_t)at * J;
         kp.err = e->d_err;
         ki.fn<<<nb, ki.threads, ki.smem, s>>>(kp);
@@ -231,7 +239,11 @@ long cf_last_launches(const cf_engine* e) { return e ? e->launches : 0; }
 uint64_t cf_workspace_bytes(int nmax, int Mmax, int J) {
     if (nmax < 1 || J < 0) return 0;
     const int F = std::max(nmax, Mmax);
-    return 8 * make_layout(nmax, F, (int)cfh::transform_length((u64)nmax), J).total;
+    const u64 L = cfh::transform_length((u64)nmax);
+    int lg = 0;
+    while ((1ull << lg) < L) ++lg;
+    if (lg > MAX_LG) return 0;
+    return 8 * make_layout(nmax, F, (int)L, J, warps_for(lg)).total;
 }
 
 long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J) {
@@ -253,7 +265,7 @@ int cf_residues_async(cf_engine* e, const uint64_t* d_primes, int B, int nmax, i
     if (rc) return rc;
     if (B == 0) return CF_OK;
     CF_CUDA(cudaSetDevice(e->device), "set device");
-    cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+    cudaStream_t s = (cudaStream_t)stream;  // NULL is the CUDA default stream
     rc = ensure_queries(e, qn, qM, J, s);
     if (rc) return rc;
     return launch_batch(e, d_primes, B, nmax, d, model, J, pl, d_residues, s);

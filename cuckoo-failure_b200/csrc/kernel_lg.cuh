@@ -23,6 +23,15 @@ struct DevExec {
     }
     __device__ __forceinline__ void sync() { __syncthreads(); }
     __device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
+    // Sum mod p of v over the calling thread's warp; lane 0 stores it at dst[warp * stride].
+    __device__ __forceinline__ void warp_sum_store(int t, u64 v, u64 P, u64* dst, size_t stride) {
+        const int T = (int)blockDim.x;
+        const unsigned mask = T >= 32 ? 0xffffffffu : ((1u << T) - 1u);
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1)
+            if (o < T) v = madd(v, __shfl_xor_sync(mask, v, o), P);
+        if ((t & 31) == 0) dst[(size_t)(t >> 5) * stride] = v;
+    }
     // red[0..T) holds values in [0, p); leaves their sum mod p in red[T].  Called by all threads.
     __device__ __forceinline__ void reduce_mod(u64* red, int T, u64 P) {
         const int t = threadIdx.x, lane = t & 31, w = t >> 5;

@@ -6,11 +6,12 @@
 // radix gives the same canonical residues after from_mont, so the choice only affects speed; the
 // reference (fast/cuckoo_fast.cu:84-99) uses R = 2^52 for its IFMA build.
 //
-// Two products are provided:
+// Products:
 //  * mont_mul(a, b): a b R^{-1} mod p, fully reduced, for inputs a, b < 2^52 (lazy inputs allowed).
 //  * shoup_mul(a, w, w'): a w mod p in [0, 2p) for a fixed multiplier w with the precomputed
-//    companion w' = floor(w 2^64 / p) (Shoup's method); a may be any 64-bit value.  Applied to a
-//    Montgomery-form w this again yields a Montgomery-form product, since w carries the factor R.
+//    companion w' = floor(w 2^64 / p) (Shoup's method); a may be any 64-bit value.
+//  * shoup_mul_lazy: the same with a cheaper quotient estimate, result in [0, 4p); the hot loops
+//    use it.  A Shoup product by a canonical constant preserves whatever form a is in.
 //
 // Primes of the fixed list have p = c 2^20 + 1 (fast/cuckoo_fast.cu:422-432).  For those, the
 // product m p needed by the reduction is m + (m c) 2^20, which saves two wide multiplies; the
@@ -108,6 +109,20 @@ CF_HD u64 shoup_companion(u64 w, u64 p) {
 #endif
 }
 
+// a w mod p in [0, 4p) for any 64-bit a, given w < p and wq = floor(w 2^64 / p).  The quotient
+// estimate keeps only the partial products of a wq that reach the high word (a1 q1 and the high
+// halves of a0 q1, a1 q0): it is at most 2 below floor(a wq / 2^64), which in turn is at most 1
+// below floor(a w / p), so the remainder lies in [0, 4p).  3 wide + 2 high + 4 low multiplies.
+CF_HD u64 shoup_mul_lazy(u64 a, u64 w, u64 wq, u64 p) {
+    const u32 a0 = lo32(a), a1 = hi32(a), q0 = lo32(wq), q1 = hi32(wq);
+#if defined(__CUDA_ARCH__)
+    const u64 q = wmul(a1, q1) + (u64)__umulhi(a0, q1) + (u64)__umulhi(a1, q0);
+#else
+    const u64 q = wmul(a1, q1) + (wmul(a0, q1) >> 32) + (wmul(a1, q0) >> 32);
+#endif
+    return a * w - q * p;  // exact modulo 2^64, and the true value is below 4p < 2^64
+}
+
 // a w mod p in [0, 2p) for any 64-bit a, given w < p and wq = floor(w 2^64 / p).
 CF_HD u64 shoup_mul(u64 a, u64 w, u64 wq, const Mod& md) {
     const u32 a0 = lo32(a), a1 = hi32(a), q0 = lo32(wq), q1 = hi32(wq);
@@ -142,7 +157,7 @@ CF_HD u64 mont_pow(u64 base, u64 e, const Mod& md) {
     }
     return r;
 }
-CF_HD u64 to_mont(u64 x, const Mod& md) { return mont_mul(x % md.p, md.r2, md); }
+CF_HD u64 to_mont(u64 x, const Mod& md) { return mont_mul(x, md.r2, md); }  // x < 2^52
 CF_HD u64 from_mont(u64 x, const Mod& md) { return mont_mul(x, 1, md); }
 
 // Per-prime constants (host or device).

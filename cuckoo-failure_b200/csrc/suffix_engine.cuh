@@ -8,8 +8,8 @@
 //
 // Design (B200, one CTA per prime, persistent over all steps v = 1 .. n-1):
 //   * the length-L transform lives in shared memory between radix-2^R register passes;
-//   * every multiplication by a constant is a Shoup product with a precomputed companion, and
-//     values stay lazily reduced in [0, 2p) / [0, 4p) inside the transforms;
+//   * every multiplication by a stored constant is a Shoup product with a precomputed companion;
+//     inside the transforms values stay lazily reduced ([0, 4p) forward, [0, 8p) inverse);
 //   * the stage factors are folded into what is stored, so stage 1 needs no multiply on input:
 //       Vs[p][w] = V[p][w] / (w! (p-1-w)! (p-1)!)        (stored V, column-major)
 //       Ss[v][q] = S[v][q] / (q! (v-q)! v!)              (stored S, column-major)
@@ -17,8 +17,11 @@
 //       stage 1:  Ss[v'][v] = D[v'-v] inv[v] conv(Vs[v][.])[v'],            D[k] = 1/k!^2
 //       stage 2:  Vs[p][v]  = g^p D[p-v-1] (D[v] - p conv(Ss[v][q] g^-q)[p])
 //       query:    out(q)    = (q-1)! sum_w Vs[q][w] / (M - w)
+//   * the powers g^p and g^-q of a step are running Montgomery products per thread (each thread
+//     holds the entries t + k T), so no per-step tables are built;
 //   * the queries are evaluated on the fly from the stage-1 input rows (the same U[w] the
-//     reference's k_query builds), so a batch needs no separate pass over V.
+//     reference's k_query builds), reduced per warp and stored per warp, so a batch needs no
+//     separate pass over V and no block barrier per row.
 //
 // The kernel code runs through an Exec policy: on the GPU `each` is the calling thread and
 // `sync` is __syncthreads; a CPU harness (tests) runs the same phases thread by thread.
@@ -35,6 +38,70 @@ enum { MODEL_SUBSET = 0, MODEL_REPLACEMENT = 1 };
 #define CF_LDG(p) (*(p))
 #endif
 
+// Scheduling controls for the hot loops.  Constant tables are interleaved (value, companion)
+// pairs fetched with one 16-byte load.  `ld_pair` is a volatile load and `pin` an empty volatile
+// statement that consumes a result: a load placed after a pin cannot be hoisted above the work
+// that produced the pinned value, which bounds how many constants are in flight (registers).
+#if defined(__CUDA_ARCH__)
+CF_HD void pin(u64& v) { asm volatile("" : "+l"(v)); }
+CF_HD void pin_int(int& v) { asm volatile("" : "+r"(v)); }
+CF_HD void ld_pair(const u64* p, u64& a, u64& b) {
+    asm volatile("ld.global.nc.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
+}
+#else
+CF_HD void pin(u64&) {}
+CF_HD void pin_int(int&) {}
+CF_HD void ld_pair(const u64* p, u64& a, u64& b) { a = p[0], b = p[1]; }
+#endif
+// Lambdas that index the register array must be inlined, or the array goes to local memory.
+#define CF_INL __attribute__((always_inline))
+// Compile-time slot index handed to the bodies below (so register-array indices are constants).
+template <int V>
+struct IC {
+    static constexpr int value = V;
+    CF_HD constexpr operator int() const { return V; }
+};
+// Unrolled loop over N units with a bounded window: body(IC<J>) pins its inputs and computes unit
+// J; done(IC<J>) pins unit J's outputs and is issued right after body(IC<J + K>).  Since volatile
+// statements keep their order, unit J + K + 1 cannot start before unit J has finished: at most
+// K + 1 units are in flight, which bounds the registers the compiler's interleaving may use.
+template <int N, int K, int J, class B, class Dn>
+CF_HD void window_step(B& body, Dn& done) {
+    if constexpr (J < N + K) {
+        if constexpr (J < N) body(IC<J>{});
+        if constexpr (J >= K && J - K < N) done(IC<J - K>{});
+        window_step<N, K, J + 1>(body, done);
+    }
+}
+template <int N, int K, class B, class Dn>
+CF_HD void window(B&& body, Dn&& done) {
+    window_step<N, K, 0>(body, done);
+}
+// Per-slot constant pairs over a window: slot J's pair addr(IC<J>) is loaded D slots ahead.
+template <int N, int D, int K, class A, class F, class Dn>
+CF_HD void pipe_pairs(A&& addr, F&& apply, Dn&& done) {
+    u64 ra[D + 1], rb[D + 1];
+    window<D, 0>([&](auto jc) CF_INL {
+        constexpr int j = decltype(jc)::value;
+        if constexpr (j < N) ld_pair(addr(jc), ra[j], rb[j]);
+    }, [&](auto) CF_INL {});
+    window<N, K>(
+        [&](auto jc) CF_INL {
+            constexpr int j = decltype(jc)::value;
+            if constexpr (j + D < N) ld_pair(addr(IC<j + D>{}), ra[(j + D) % (D + 1)], rb[(j + D) % (D + 1)]);
+            apply(jc, ra[j % (D + 1)], rb[j % (D + 1)]);
+        },
+        done);
+}
+#ifndef CF_PIPE_D
+#define CF_PIPE_D 4
+#endif
+#ifndef CF_WIN_K
+#define CF_WIN_K 3
+#endif
+constexpr int PIPE_D = CF_PIPE_D;  // constants loaded ahead
+constexpr int WIN_K = CF_WIN_K;    // units in flight beyond the current one
+
 // Transform geometry: L = 2^LG entries, T threads holding E = 2^R entries each.  The LG levels
 // are done in passes of R levels (the last pass may have fewer); between passes the entries go
 // through shared memory.
@@ -44,9 +111,7 @@ struct Geo {
     static constexpr int L = 1 << LG, E = 1 << R, T = 1 << (LG - R);
     static constexpr int NP = (LG + R - 1) / R;  // number of passes
     static constexpr int SWZ = R > 4 ? R : 4;    // shared-memory swizzle shift
-    static constexpr int HLO = (LG + 1) / 2;     // two-level power tables: x^e = hi[e >> HLO] lo[e & (LO-1)]
-    static constexpr int LO = 1 << HLO, HI = (L >> HLO) + 1;
-    static constexpr int GT = LO > HI ? LO : HI;  // entries per power table
+    static constexpr int NW = (T + 31) / 32;     // warps
     CF_HD static constexpr int pass_b(int p) { return LG - (p + 1) * R > 0 ? LG - (p + 1) * R : 0; }
     CF_HD static constexpr int pass_r(int p) { return LG - p * R - pass_b(p); }
     // index of the entry held in slot j by thread t during pass p
@@ -61,33 +126,29 @@ struct Geo {
 CF_HD u64 red2(u64 x, u64 m) { return x >= m ? x - m : x; }  // [0, 2m) -> [0, m)
 
 // Per-prime global workspace, in 64-bit words (every table 256-byte aligned).
+// Tables marked "pairs" hold (value, Shoup companion) interleaved: entry k at [2k], [2k+1].
 struct Layout {
-    size_t V, S, fact, factq, ifact, ifactq, inv, invq, D, Dq, Kq, W, Wq, hat, hatq, ps, total;
+    size_t V, S, fact, ifact, inv, D, Kq, W, hat, ps, total;
 };
 CF_HD size_t lay_take(size_t& at, size_t cnt) {
     const size_t r = at;
     at += (cnt + 31) & ~(size_t)31;
     return r;
 }
-CF_HD Layout make_layout(int n, int F, int L, int J) {
+// nw = warps per CTA: query partial sums are kept per warp.
+CF_HD Layout make_layout(int n, int F, int L, int J, int nw) {
     Layout o;
     size_t at = 0;
     o.V = lay_take(at, (size_t)n * (n + 1) / 2);  // columns w = 0..n-1, rows p = w+1..n
     o.S = lay_take(at, (size_t)n * (n - 1) / 2);  // columns q = 1..n-1, rows v = q..n-1
-    o.fact = lay_take(at, (size_t)F + 1);
-    o.factq = lay_take(at, (size_t)F + 1);
-    o.ifact = lay_take(at, (size_t)F + 1);
-    o.ifactq = lay_take(at, (size_t)F + 1);
-    o.inv = lay_take(at, (size_t)F + 1);
-    o.invq = lay_take(at, (size_t)F + 1);
-    o.D = lay_take(at, (size_t)n + 1);
-    o.Dq = lay_take(at, (size_t)n + 1);
-    o.Kq = lay_take(at, (size_t)n + 1);
-    o.W = lay_take(at, (size_t)L / 2 + 1);
-    o.Wq = lay_take(at, (size_t)L / 2 + 1);
-    o.hat = lay_take(at, (size_t)L);
-    o.hatq = lay_take(at, (size_t)L);
-    o.ps = lay_take(at, (size_t)J * (n + 1));
+    o.fact = lay_take(at, 2 * ((size_t)F + 1));   // pairs: k!
+    o.ifact = lay_take(at, 2 * ((size_t)F + 1));  // pairs: 1/k!
+    o.inv = lay_take(at, 2 * ((size_t)F + 1));    // pairs: 1/k
+    o.D = lay_take(at, 2 * ((size_t)n + 1));      // pairs: 1/k!^2
+    o.Kq = lay_take(at, (size_t)n + 1);           // companions of the integers k
+    o.W = lay_take(at, 2 * ((size_t)L / 2 + 1));  // pairs: w^k, w of order L
+    o.hat = lay_take(at, 2 * (size_t)L);          // pairs: spectrum of the kernel 1/t, times 1/L
+    o.ps = lay_take(at, (size_t)J * nw * (n + 1));  // [J][nw][n+1]
     o.total = at;
     return o;
 }
@@ -102,23 +163,24 @@ struct KParams {
     const int* qM;      // [J] query table sizes M_j <= F
     u64* ws;            // workspace base
     size_t ws_words;    // words per prime
+    Layout lay;         // offsets inside a prime's workspace
     u64* out;           // [B][J] residues
     int* err;           // device error word (0 = ok)
 };
 
 // Error codes recorded in *err by the kernel.
-enum { KERR_NONE = 0, KERR_NO_ROOT = 1, KERR_BOUNDS = 2 };
+enum { KERR_NONE = 0, KERR_NO_ROOT = 1 };
 
 // Shared memory per CTA, in 64-bit words.
 template <class G>
 struct Smem {
     static constexpr int X = 0;                       // [L] transform exchange (swizzled)
     static constexpr int RED = G::L;                  // [2T + 64] reduction and scan scratch
-    static constexpr int TAB = RED + 2 * G::T + 64;   // [8][GT] power tables and companions
-    static constexpr int MISC = TAB + 8 * G::GT;      // [16] scalars
+    static constexpr int MISC = RED + 2 * G::T + 64;  // [16] modulus constants and scalars
     static constexpr int WORDS = MISC + 16;
     static constexpr size_t BYTES = (size_t)WORDS * 8;
 };
+enum { MI_P = 0, MI_PINV = 1, MI_R1 = 2, MI_R2 = 3, MI_ONEQ = 4, MI_ROOT = 5, MI_LINV = 6 };
 
 template <class G>
 struct Regs {
@@ -127,105 +189,143 @@ struct Regs {
 
 template <class G, class X>
 struct PrimeRun {
-    static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP;
+    static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP, NW = G::NW;
     X& ex;
     const KParams& kp;
-    int b;  // prime index within the batch
-    u64 P, P2, one_q;  // one_q = floor(2^64 / p): Shoup companion of 1, reduces any 64-bit value to [0, 2p)
-    Mod md;
-    int n, F, d, d0, model, J;
-    u64 *V, *S, *fact, *factq, *ifact, *ifactq, *inv, *invq, *D, *Dq, *Kq, *W, *Wq, *hat, *hatq, *ps;
-    u64* sm;
+    int b;      // prime index within the batch
+    u64* base;  // this prime's workspace
+    u64* sm;    // shared memory
+    u64 P;
 
     CF_HD PrimeRun(X& e, const KParams& k, int bi, u64* smem) : ex(e), kp(k), b(bi), sm(smem) {
         P = kp.primes[b];
-        P2 = 2 * P;
-        md = make_mod(P);
-        one_q = shoup_companion(1, P);
-        n = kp.n, F = kp.F, d = kp.d, d0 = kp.d0, model = kp.model, J = kp.J;
-        const Layout lo = make_layout(n, F, L, J);
-        u64* base = kp.ws + (size_t)b * kp.ws_words;
-        V = base + lo.V, S = base + lo.S;
-        fact = base + lo.fact, factq = base + lo.factq, ifact = base + lo.ifact, ifactq = base + lo.ifactq;
-        inv = base + lo.inv, invq = base + lo.invq, D = base + lo.D, Dq = base + lo.Dq, Kq = base + lo.Kq;
-        W = base + lo.W, Wq = base + lo.Wq, hat = base + lo.hat, hatq = base + lo.hatq, ps = base + lo.ps;
+        base = kp.ws + (size_t)b * kp.ws_words;
+    }
+    // workspace tables (offsets live in the kernel parameters, so these hold no registers)
+    CF_HD u64* V() const { return base + kp.lay.V; }
+    CF_HD u64* S() const { return base + kp.lay.S; }
+    CF_HD u64* fact() const { return base + kp.lay.fact; }
+    CF_HD u64* ifact() const { return base + kp.lay.ifact; }
+    CF_HD u64* inv() const { return base + kp.lay.inv; }
+    CF_HD u64* D() const { return base + kp.lay.D; }
+    CF_HD u64* Kq() const { return base + kp.lay.Kq; }
+    CF_HD u64* W() const { return base + kp.lay.W; }
+    CF_HD u64* hat() const { return base + kp.lay.hat; }
+    CF_HD u64* ps() const { return base + kp.lay.ps; }
+    CF_HD u64* misc() const { return sm + Smem<G>::MISC; }
+    CF_HD Mod md() const {  // modulus constants, kept in shared memory
+        const u64* m = misc();
+        Mod r;
+        r.p = m[MI_P], r.pinv = m[MI_PINV], r.r1 = m[MI_R1], r.r2 = m[MI_R2];
+        return r;
     }
 
-    CF_HD u64 sh(u64 a, const u64* tab, const u64* tabq, int k) const {  // a * tab[k] via Shoup
-        return shoup_mul(a, CF_LDG(tab + k), CF_LDG(tabq + k), md);
+    CF_HD u64 sh(u64 a, const u64* pairs, int k) const {  // a * pairs[k], result in [0, 4p)
+        return shoup_mul_lazy(a, CF_LDG(pairs + 2 * k), CF_LDG(pairs + 2 * k + 1), P);
     }
-    CF_HD u64 canon_mul(u64 a, u64 bb) const { return mont_mul(mont_mul(a, bb, md), md.r2, md); }  // a b mod p, canonical
+    CF_HD static void put_pair(u64* pairs, int k, u64 v, u64 P) {
+        pairs[2 * k] = v;
+        pairs[2 * k + 1] = shoup_companion(v, P);
+    }
+    CF_HD u64 canon(u64 x) const { return red2(red2(x, 2 * P), P); }  // [0, 4p) -> [0, p)
 
     // ---------------------------------------------------------------------------------------
     // Transform passes.  Forward: Gentleman-Sande (natural in, bit-reversed out); inverse:
     // Cooley-Tukey with inverse roots (bit-reversed in, natural out, unscaled), the same pair of
     // transforms as fast/cuckoo_fast.cu:258-305 and include/cuckoo/ntt.hpp:97-123.  W[k] = w^k
     // for k <= L/2 (W[L/2] = -1), so w_{2h}^{-j} = -W[L/2 - j L/2h] for every j, including 0.
+    // Forward values stay in [0, 4p), inverse values in [0, 8p).
     // ---------------------------------------------------------------------------------------
-    template <int PASS>
-    CF_HD void fwd_pass(int t, u64 (&x)[E]) const {
-        constexpr int bb = G::pass_b(PASS), r = G::pass_r(PASS);
-        const int off = bb ? (t & ((1 << bb) - 1)) : 0;
-#pragma unroll
-        for (int m = r - 1; m >= 0; --m) {
-            const int shift = G::LG - 1 - bb - m;
-#pragma unroll
-            for (int ul = 0; ul < (1 << m); ++ul) {
-                const bool trivial = (bb == 0 && ul == 0);
-                u64 w = 1, wq = 0;
-                if (!trivial) {
-                    const int k = (off + (ul << bb)) << shift;
-                    w = CF_LDG(W + k), wq = CF_LDG(Wq + k);
-                }
-#pragma unroll
-                for (int s = 0; s < (E >> r); ++s)
-#pragma unroll
-                    for (int uh = 0; uh < (1 << (r - 1 - m)); ++uh) {
-                        const int j0 = (s << r) + (uh << (m + 1)) + ul, j1 = j0 + (1 << m);
-                        const u64 a = x[j0], c = x[j1];
-                        x[j0] = red2(a + c, P2);
-                        const u64 dd = a - c + P2;
-                        x[j1] = trivial ? red2(dd, P2) : shoup_mul(dd, w, wq, md);
-                    }
-            }
+    // Butterfly schedule of one register pass.  Unit q runs in order of level (forward: m = r-1
+    // down to 0; inverse: 0 up), then twiddle group (ul), then register pair; grp(q) numbers the
+    // twiddle groups in that order.
+    template <int PASS, bool FWD>
+    struct Plan {
+        static constexpr int bb = G::pass_b(PASS), r = G::pass_r(PASS);
+        static constexpr int BPL = E / 2, NB = BPL * r, NG = (1 << r) - 1;
+        CF_HD static constexpr int m(int q) { return FWD ? r - 1 - q / BPL : q / BPL; }
+        CF_HD static constexpr int per(int q) { return E >> (m(q) + 1); }  // butterflies per group
+        CF_HD static constexpr int ul(int q) { return (q % BPL) / per(q); }
+        CF_HD static constexpr int kk(int q) { return (q % BPL) % per(q); }
+        CF_HD static constexpr int grp(int q) { return FWD ? (1 << r) - (1 << (m(q) + 1)) + ul(q) : (1 << m(q)) - 1 + ul(q); }
+        CF_HD static constexpr int j0(int q) {
+            return ((kk(q) >> (r - 1 - m(q))) << r) + ((kk(q) & ((1 << (r - 1 - m(q))) - 1)) << (m(q) + 1)) + ul(q);
         }
+        CF_HD static constexpr int j1(int q) { return j0(q) + (1 << m(q)); }
+        // level and group-within-level of twiddle group f
+        CF_HD static constexpr int gm(int f) {
+            int mm = FWD ? r - 1 : 0;
+            while (f >= (1 << mm)) f -= (1 << mm), mm += FWD ? -1 : 1;
+            return mm;
+        }
+        CF_HD static constexpr int gul(int f) {
+            int mm = FWD ? r - 1 : 0;
+            while (f >= (1 << mm)) f -= (1 << mm), mm += FWD ? -1 : 1;
+            return f;
+        }
+        CF_HD static constexpr bool trivial_grp(int f) { return bb == 0 && gul(f) == 0; }
+    };
+    // pair address of the twiddle of group F (forward: w_{2h}^j; inverse: W[L/2 - j L/2h], whose
+    // negation is w_{2h}^{-j})
+    template <int PASS, bool FWD, int F>
+    CF_HD const u64* tw_addr(int off) const {
+        typedef Plan<PASS, FWD> PL;
+        constexpr int mm = PL::gm(F), ul = PL::gul(F);
+        const int j = (off + (ul << PL::bb)) << (G::LG - 1 - PL::bb - mm);
+        return W() + 2 * (FWD ? j : L / 2 - j);
+    }
+    template <int PASS, bool FWD>
+    CF_HD void pass(int t, u64 (&x)[E]) const {
+        typedef Plan<PASS, FWD> PL;
+        constexpr int D = PIPE_D;
+        const int off = PL::bb ? (t & ((1 << PL::bb) - 1)) : 0;
+        const u64 P4 = 4 * P;
+        u64 rw[D + 1], rq[D + 1];
+        window<D, 0>([&](auto fc) CF_INL {
+            constexpr int f = decltype(fc)::value;
+            if constexpr (f < PL::NG && !PL::trivial_grp(f)) ld_pair(tw_addr<PASS, FWD, f>(off), rw[f], rq[f]);
+        }, [&](auto) CF_INL {});
+        window<PL::NB, WIN_K>(
+            [&](auto qc) CF_INL {
+                constexpr int q = decltype(qc)::value, f = PL::grp(q), fn = f + D;
+                if constexpr (PL::kk(q) == 0 && fn < PL::NG && !PL::trivial_grp(fn))
+                    ld_pair(tw_addr<PASS, FWD, fn>(off), rw[fn % (D + 1)], rq[fn % (D + 1)]);
+                constexpr int j0 = PL::j0(q), j1 = PL::j1(q);
+                constexpr bool trivial = PL::trivial_grp(f);
+                pin(x[j0]);
+                pin(x[j1]);
+                const u64 w = rw[f % (D + 1)], wq = rq[f % (D + 1)];
+                if constexpr (FWD) {
+                    const u64 a = x[j0], c = x[j1];
+                    x[j0] = red2(a + c, P4);
+                    const u64 dd = a - c + P4;
+                    x[j1] = trivial ? red2(dd, P4) : shoup_mul_lazy(dd, w, wq, P);
+                } else {
+                    const u64 a = red2(x[j0], P4);
+                    if constexpr (trivial) {
+                        const u64 c = red2(x[j1], P4);
+                        x[j0] = a + c;
+                        x[j1] = a - c + P4;
+                    } else {
+                        const u64 c = shoup_mul_lazy(x[j1], w, wq, P);  // -w_{2h}^{-j} y
+                        x[j0] = a - c + P4;
+                        x[j1] = a + c;
+                    }
+                }
+            },
+            [&](auto qc) CF_INL {
+                constexpr int q = decltype(qc)::value;
+                pin(x[PL::j0(q)]);
+                pin(x[PL::j1(q)]);
+            });
     }
     template <int PASS>
-    CF_HD void inv_pass(int t, u64 (&x)[E]) const {
-        constexpr int bb = G::pass_b(PASS), r = G::pass_r(PASS);
-        const int off = bb ? (t & ((1 << bb) - 1)) : 0;
-#pragma unroll
-        for (int m = 0; m < r; ++m) {
-            const int shift = G::LG - 1 - bb - m;
-#pragma unroll
-            for (int ul = 0; ul < (1 << m); ++ul) {
-                const bool trivial = (bb == 0 && ul == 0);
-                u64 w = 1, wq = 0;
-                if (!trivial) {
-                    const int k = (L / 2) - ((off + (ul << bb)) << shift);
-                    w = CF_LDG(W + k), wq = CF_LDG(Wq + k);
-                }
-#pragma unroll
-                for (int s = 0; s < (E >> r); ++s)
-#pragma unroll
-                    for (int uh = 0; uh < (1 << (r - 1 - m)); ++uh) {
-                        const int j0 = (s << r) + (uh << (m + 1)) + ul, j1 = j0 + (1 << m);
-                        const u64 a = red2(x[j0], P2);
-                        if (trivial) {
-                            const u64 c = red2(x[j1], P2);
-                            x[j0] = a + c;
-                            x[j1] = a - c + P2;
-                        } else {
-                            const u64 c = shoup_mul(x[j1], w, wq, md);  // -w_{2h}^{-j} y
-                            x[j0] = a - c + P2;
-                            x[j1] = a + c;
-                        }
-                    }
-            }
-        }
-    }
+    CF_HD void fwd_pass(int t, u64 (&x)[E]) const { pass<PASS, true>(t, x); }
+    template <int PASS>
+    CF_HD void inv_pass(int t, u64 (&x)[E]) const { pass<PASS, false>(t, x); }
     template <int PASS>
     CF_HD void to_smem(int t, const u64 (&x)[E]) const {
+        pin_int(t);  // recompute the addresses rather than keep the loads' 32 addresses live across the pass
 #pragma unroll
         for (int j = 0; j < E; ++j) sm[G::swz(G::idx(PASS, t, j))] = x[j];
     }
@@ -236,23 +336,23 @@ struct PrimeRun {
     }
 
     template <int PASS>
-    CF_HD void fwd_chain() {  // passes PASS .. NP-1 of the forward transform (entry: data in smem, PASS >= 1)
+    CF_HD void fwd_chain() {  // forward passes PASS .. NP-1, pointwise, last inverse pass (PASS >= 1)
         ex.sync();
-        ex.each([&](int t, Regs<G>& rg) {
+        ex.each([&](int t, Regs<G>& rg) CF_INL {
             from_smem<PASS>(t, rg.x);
             fwd_pass<PASS>(t, rg.x);
             if (PASS == NP - 1) {
                 pointwise(t, rg.x);
                 inv_pass<PASS>(t, rg.x);
             }
-            if (PASS > 0) to_smem<PASS>(t, rg.x);
+            to_smem<PASS>(t, rg.x);
         });
         if constexpr (PASS + 1 < NP) fwd_chain<PASS + 1>();
     }
     template <int PASS>
-    CF_HD void inv_chain() {  // inverse passes PASS .. 0 (entry: data in smem in layout PASS)
+    CF_HD void inv_chain() {  // inverse passes PASS .. 0 (entry: data in smem in layout PASS + 1)
         ex.sync();
-        ex.each([&](int t, Regs<G>& rg) {
+        ex.each([&](int t, Regs<G>& rg) CF_INL {
             from_smem<PASS>(t, rg.x);
             inv_pass<PASS>(t, rg.x);
             if (PASS > 0) to_smem<PASS>(t, rg.x);
@@ -260,23 +360,27 @@ struct PrimeRun {
         if constexpr (PASS > 0) inv_chain<PASS - 1>();
     }
     CF_HD void pointwise(int t, u64 (&x)[E]) const {
-#pragma unroll
-        for (int j = 0; j < E; ++j) {
-            const int i = G::idx(NP - 1, t, j);
-            x[j] = sh(x[j], hat, hatq, i);
-        }
+        const u64* h = hat();
+        pipe_pairs<E, PIPE_D, WIN_K>(
+            [&](auto jc) CF_INL { return h + 2 * G::idx(NP - 1, t, decltype(jc)::value); },
+            [&](auto jc, u64 w, u64 wq) CF_INL {
+                constexpr int j = decltype(jc)::value;
+                pin(x[j]);
+                x[j] = shoup_mul_lazy(x[j], w, wq, P);
+            },
+            [&](auto jc) CF_INL { pin(x[decltype(jc)::value]); });
     }
-    // Cyclic convolution of the registers (layout of pass 0) with the kernel 1/t; the result comes
-    // back in the same layout, in [0, 4p).
+    // Cyclic convolution of the registers (layout of pass 0, values < 4p) with the kernel 1/t;
+    // the result comes back in the same layout, in [0, 8p).
     CF_HD void convolve() {
         if constexpr (NP == 1) {
-            ex.each([&](int t, Regs<G>& rg) {
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
                 fwd_pass<0>(t, rg.x);
                 pointwise(t, rg.x);
                 inv_pass<0>(t, rg.x);
             });
         } else {
-            ex.each([&](int t, Regs<G>& rg) {
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
                 fwd_pass<0>(t, rg.x);
                 to_smem<0>(t, rg.x);
             });
@@ -284,179 +388,12 @@ struct PrimeRun {
             inv_chain<NP - 2>();
         }
     }
-
-    // ---------------------------------------------------------------------------------------
-    // Block reduction of per-thread values mod p: each thread leaves its value in RED[t].
-    // ---------------------------------------------------------------------------------------
-    CF_HD u64 sum_red() {
-        u64* red = sm + Smem<G>::RED;
-        ex.sync();
-        ex.reduce_mod(red, T, P);  // leaves the total in red[0] (and in red[T] for all readers)
-        ex.sync();
-        const u64 s = red[T];
-        return s;
-    }
-
-    // Powers x^e for 0 <= e < L through two tables: tab[0..GT) = x^(j), tab[2GT..) = x^(j LO).
-    // Companions in the odd slots.  xm is x in Montgomery form.  Called by every thread.
-    CF_HD void power_tables(int t, u64 xm, u64* tab) const {
-        for (int k = t; k < G::LO + G::HI; k += T) {
-            const bool lo = k < G::LO;
-            const u64 e = lo ? (u64)k : (u64)(k - G::LO) << G::HLO;
-            const u64 v = from_mont(mont_pow(xm, e, md), md);
-            u64* dst = lo ? tab + k : tab + 2 * G::GT + (k - G::LO);
-            dst[0] = v;
-            dst[G::GT] = shoup_companion(v, P);
-        }
-    }
-    // x^e for e < L from the tables (canonical, [0, 2p) lazily) times a
-    CF_HD u64 mul_pow(u64 a, const u64* tab, int e) const {
-        const int lo = e & (G::LO - 1), hi = e >> G::HLO;
-        a = shoup_mul(a, tab[lo], tab[G::GT + lo], md);
-        return shoup_mul(a, tab[2 * G::GT + hi], tab[3 * G::GT + hi], md);
-    }
-
-    // g(v) in Montgomery form, and 1/g(v) (g != 0 for v >= d0)
-    CF_HD u64 g_mont(int v) const {
-        if (model == MODEL_REPLACEMENT) return mont_pow(to_mont((u64)v, md), (u64)d, md);
-        const u64 c = red2(sh(sh(CF_LDG(fact + v), ifact, ifactq, d), ifact, ifactq, v - d), P);
-        return to_mont(c, md);
-    }
-    CF_HD u64 ginv_mont(int v) const {
-        if (model == MODEL_REPLACEMENT) return mont_pow(to_mont(CF_LDG(inv + v), md), (u64)d, md);
-        const u64 c = red2(sh(sh(CF_LDG(ifact + v), fact, factq, d), fact, factq, v - d), P);
-        return to_mont(c, md);
-    }
-
-    // ---------------------------------------------------------------------------------------
-    // Setup: factorials, inverses, D, twiddles and the kernel spectrum of 1/t (the per-batch host
-    // work of fast/cuckoo_fast.cu:797-839, done on the device).
-    // ---------------------------------------------------------------------------------------
-    CF_HD void setup() {
-        u64* red = sm + Smem<G>::RED;  // red[t]: prefix before chunk t; red[T + t]: chunk product / suffix
-        u64* misc = sm + Smem<G>::MISC;
-        const int C = (F + 1 + T - 1) / T;  // factorial entries k = 0..F, chunk of C per thread
-        // product of the integers in each chunk (Montgomery form)
-        ex.each([&](int t, Regs<G>&) {
-            const int k0 = t * C > 1 ? t * C : 1, k1 = (t + 1) * C < F + 1 ? (t + 1) * C : F + 1;
-            u64 pr = md.r1;
-            u64 km = to_mont((u64)k0, md);
-            for (int k = k0; k < k1; ++k) {
-                pr = mont_mul(pr, km, md);
-                km = madd(km, md.r1, P);
-            }
-            red[T + t] = pr;
-        });
-        ex.sync();
-        ex.single([&]() {  // exclusive prefix products, F!, 1/F!, exclusive suffix products / F!
-            u64 run = md.r1;
-            for (int t = 0; t < T; ++t) {
-                red[t] = run;
-                run = mont_mul(run, red[T + t], md);
-            }
-            u64 suf = mont_pow(run, P - 2, md);  // 1/F!
-            for (int t = T - 1; t >= 0; --t) {
-                const u64 c = red[T + t];
-                red[T + t] = suf;  // 1/F! times the product of the chunks after t = 1/(last k of chunk t)!
-                suf = mont_mul(suf, c, md);
-            }
-        });
-        ex.sync();
-        ex.each([&](int t, Regs<G>&) {
-            const int k0 = t * C, k1 = (t + 1) * C < F + 1 ? (t + 1) * C : F + 1;
-            u64 run = red[t];  // (k0 - 1)! (Montgomery), 1 for the first chunk
-            u64 km = to_mont((u64)(k0 > 0 ? k0 : 1), md);
-            for (int k = k0; k < k1; ++k) {  // k! = (k-1)! k
-                if (k > 0) {
-                    run = mont_mul(run, km, md);
-                    km = madd(km, md.r1, P);
-                }
-                const u64 c = from_mont(run, md);
-                fact[k] = c;
-                factq[k] = shoup_companion(c, P);
-            }
-            run = red[T + t];  // 1/(k1 - 1)!
-            for (int k = k1 - 1; k >= k0; --k) {  // 1/(k-1)! = k / k!
-                const u64 c = from_mont(run, md);
-                ifact[k] = c;
-                ifactq[k] = shoup_companion(c, P);
-                if (k > 0) run = mont_mul(run, to_mont((u64)k, md), md);
-            }
-        });
-        ex.sync();
-        // inv[k] = (k-1)!/k!, D[k] = 1/k!^2, Kq[k] = companion of k
-        ex.each([&](int t, Regs<G>&) {
-            for (int k = t; k <= F; k += T) {
-                const u64 c = k ? red2(sh(CF_LDG(ifact + k), fact, factq, k - 1), P) : 0;
-                inv[k] = c;
-                invq[k] = shoup_companion(c, P);
-            }
-            for (int k = t; k <= n; k += T) {
-                const u64 ik = CF_LDG(ifact + k);
-                const u64 c = red2(sh(ik, ifact, ifactq, k), P);
-                D[k] = c;
-                Dq[k] = shoup_companion(c, P);
-                Kq[k] = shoup_companion((u64)k % P, P);
-            }
-            for (int q = 0; q < J; ++q)
-                for (int k = t; k <= n; k += T) ps[(size_t)q * (n + 1) + k] = 0;
-        });
-        // a root of unity of order L: x^((p-1)/L) whose (L/2)-th power is -1 (fast/cuckoo_fast.cu:815-820)
-        ex.single([&]() {
-            const u64 minus1 = P - md.r1;
-            u64 w = 0;
-            int found = 0;
-            for (u64 x = 2; x < 1000; ++x) {
-                w = mont_pow(to_mont(x, md), (P - 1) / L, md);
-                if (mont_pow(w, L / 2, md) == minus1) {
-                    found = 1;
-                    break;
-                }
-            }
-            if (!found) ex.set_error(kp.err, KERR_NO_ROOT);
-            misc[2] = w;
-            misc[3] = mont_pow(to_mont((u64)L, md), P - 2, md);  // 1/L (Montgomery)
-        });
-        ex.sync();
-        ex.each([&](int t, Regs<G>&) {
-            const u64 w = misc[2];
-            u64 cur = mont_pow(w, (u64)t, md);
-            const u64 step = mont_pow(w, (u64)T, md);
-            for (int k = t; k <= L / 2; k += T) {
-                const u64 c = from_mont(cur, md);
-                W[k] = c;
-                Wq[k] = shoup_companion(c, P);
-                cur = mont_mul(cur, step, md);
-            }
-        });
-        ex.sync();
-        // kernel spectrum: hat = DIF(ker) / L with ker[t] = 1/t for 1 <= t <= n-1 (fast/cuckoo_fast.cu:829,838-839)
-        ex.each([&](int t, Regs<G>& rg) {
-#pragma unroll
-            for (int j = 0; j < E; ++j) {
-                const int i = G::idx(0, t, j);
-                rg.x[j] = (i >= 1 && i < n) ? CF_LDG(inv + i) : 0;
-            }
-        });
-        fwd_only();
-        ex.each([&](int t, Regs<G>& rg) {
-            const u64 linv = from_mont(misc[3], md);
-            const u64 linvq = shoup_companion(linv, P);
-#pragma unroll
-            for (int j = 0; j < E; ++j) {
-                const int i = G::idx(NP - 1, t, j);
-                const u64 c = red2(shoup_mul(rg.x[j], linv, linvq, md), P);
-                hat[i] = c;
-                hatq[i] = shoup_companion(c, P);
-            }
-        });
-        ex.sync();
-    }
-    // forward transform only (registers in layout 0 -> registers in layout NP-1)
+    // forward transform only (registers in layout 0 -> registers in layout NP-1), used for the
+    // kernel spectrum
     template <int PASS>
     CF_HD void fwd_only_chain() {
         ex.sync();
-        ex.each([&](int t, Regs<G>& rg) {
+        ex.each([&](int t, Regs<G>& rg) CF_INL {
             from_smem<PASS>(t, rg.x);
             fwd_pass<PASS>(t, rg.x);
             if (PASS < NP - 1) to_smem<PASS>(t, rg.x);
@@ -465,9 +402,9 @@ struct PrimeRun {
     }
     CF_HD void fwd_only() {
         if constexpr (NP == 1) {
-            ex.each([&](int t, Regs<G>& rg) { fwd_pass<0>(t, rg.x); });
+            ex.each([&](int t, Regs<G>& rg) CF_INL { fwd_pass<0>(t, rg.x); });
         } else {
-            ex.each([&](int t, Regs<G>& rg) {
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
                 fwd_pass<0>(t, rg.x);
                 to_smem<0>(t, rg.x);
             });
@@ -475,134 +412,316 @@ struct PrimeRun {
         }
     }
 
+    // Block sum mod p of the values the threads left in RED[t] (returned to every thread).
+    CF_HD u64 sum_red() {
+        u64* red = sm + Smem<G>::RED;
+        ex.sync();
+        ex.reduce_mod(red, T, P);
+        ex.sync();
+        return red[T];
+    }
+
+    // value of a pair table, canonical
+    CF_HD static u64 val(const u64* pairs, int k) { return CF_LDG(pairs + 2 * k); }
+
+    // g(v) and 1/g(v) in Montgomery form (g != 0 for v >= d0)
+    CF_HD u64 g_mont(int v, const Mod& m) const {
+        if (kp.model == MODEL_REPLACEMENT) return mont_pow(to_mont((u64)v, m), (u64)kp.d, m);
+        return to_mont(canon(sh(sh(val(fact(), v), ifact(), kp.d), ifact(), v - kp.d)), m);  // C(v, d)
+    }
+    CF_HD u64 ginv_mont(int v, const Mod& m) const {
+        if (kp.model == MODEL_REPLACEMENT) return mont_pow(to_mont(val(inv(), v), m), (u64)kp.d, m);
+        return to_mont(canon(sh(sh(val(ifact(), v), fact(), kp.d), fact(), v - kp.d)), m);
+    }
+
     // ---------------------------------------------------------------------------------------
-    // Query partial sums for row q: ps_j[q] = sum_{w<q} Vs[q][w] / (M_j - w), for every query
-    // with n_j >= q (the U[w] / (M - w) sums of fast/cuckoo_fast.cu:306-323, 595-622).
-    // The row must be in the registers (layout 0, entries w >= q zero).
+    // Setup: factorials, inverses, D, twiddles and the kernel spectrum of 1/t (the per-batch host
+    // work of fast/cuckoo_fast.cu:797-839, done on the device).
+    // ---------------------------------------------------------------------------------------
+    CF_HD void setup() {
+        u64* red = sm + Smem<G>::RED;  // red[t]: prefix before chunk t; red[T + t]: chunk product / suffix
+        u64* mi = misc();
+        const int F = kp.F, n = kp.n, J = kp.J;
+        ex.single([&]() CF_INL {
+            const Mod m = make_mod(P);
+            mi[MI_P] = m.p, mi[MI_PINV] = m.pinv, mi[MI_R1] = m.r1, mi[MI_R2] = m.r2;
+            mi[MI_ONEQ] = shoup_companion(1, P);
+        });
+        ex.sync();
+        const int C = (F + 1 + T - 1) / T;  // factorial entries k = 0..F, chunk of C per thread
+        // product of the integers in each chunk (Montgomery form)
+        ex.each([&](int t, Regs<G>&) CF_INL {
+            const Mod m = md();
+            const int k0 = t * C > 1 ? t * C : 1, k1 = (t + 1) * C < F + 1 ? (t + 1) * C : F + 1;
+            u64 pr = m.r1;
+            u64 km = to_mont((u64)k0, m);
+            for (int k = k0; k < k1; ++k) {
+                pr = mont_mul(pr, km, m);
+                km = madd(km, m.r1, P);
+            }
+            red[T + t] = pr;
+        });
+        ex.sync();
+        ex.single([&]() CF_INL {  // exclusive prefix products, F!, 1/F!, exclusive suffix products / F!
+            const Mod m = md();
+            u64 run = m.r1;
+            for (int t = 0; t < T; ++t) {
+                red[t] = run;
+                run = mont_mul(run, red[T + t], m);
+            }
+            u64 suf = mont_pow(run, P - 2, m);  // 1/F!
+            for (int t = T - 1; t >= 0; --t) {
+                const u64 c = red[T + t];
+                red[T + t] = suf;  // 1/F! times the product of the chunks after t = 1/(last k of chunk t)!
+                suf = mont_mul(suf, c, m);
+            }
+        });
+        ex.sync();
+        ex.each([&](int t, Regs<G>&) CF_INL {
+            const Mod m = md();
+            const int k0 = t * C, k1 = (t + 1) * C < F + 1 ? (t + 1) * C : F + 1;
+            u64 run = red[t];  // (k0 - 1)! (Montgomery), 1 for the first chunk
+            u64 km = to_mont((u64)(k0 > 0 ? k0 : 1), m);
+            for (int k = k0; k < k1; ++k) {  // k! = (k-1)! k
+                if (k > 0) {
+                    run = mont_mul(run, km, m);
+                    km = madd(km, m.r1, P);
+                }
+                put_pair(fact(), k, from_mont(run, m), P);
+            }
+            run = red[T + t];  // 1/(k1 - 1)!
+            for (int k = k1 - 1; k >= k0; --k) {  // 1/(k-1)! = k / k!
+                put_pair(ifact(), k, from_mont(run, m), P);
+                if (k > 0) run = mont_mul(run, to_mont((u64)k, m), m);
+            }
+        });
+        ex.sync();
+        // inv[k] = (k-1)!/k!, D[k] = 1/k!^2, Kq[k] = companion of k; query partial sums zeroed
+        ex.each([&](int t, Regs<G>&) CF_INL {
+            for (int k = t; k <= F; k += T) put_pair(inv(), k, k ? canon(sh(val(ifact(), k), fact(), k - 1)) : 0, P);
+            for (int k = t; k <= n; k += T) {
+                put_pair(D(), k, canon(sh(val(ifact(), k), ifact(), k)), P);
+                Kq()[k] = shoup_companion((u64)k, P);
+            }
+            const size_t nps = (size_t)J * NW * (n + 1);
+            for (size_t k = t; k < nps; k += T) ps()[k] = 0;
+        });
+        // a root of unity of order L: x^((p-1)/L) whose (L/2)-th power is -1 (fast/cuckoo_fast.cu:815-820)
+        ex.single([&]() CF_INL {
+            const Mod m = md();
+            const u64 minus1 = P - m.r1;
+            u64 w = 0;
+            int found = 0;
+            for (u64 x = 2; x < 1000; ++x) {
+                w = mont_pow(to_mont(x, m), (P - 1) / L, m);
+                if (mont_pow(w, L / 2, m) == minus1) {
+                    found = 1;
+                    break;
+                }
+            }
+            if (!found) ex.set_error(kp.err, KERR_NO_ROOT);
+            mi[MI_ROOT] = w;
+            mi[MI_LINV] = from_mont(mont_pow(to_mont((u64)L, m), P - 2, m), m);  // 1/L, canonical
+        });
+        ex.sync();
+        ex.each([&](int t, Regs<G>&) CF_INL {
+            const Mod m = md();
+            const u64 w = mi[MI_ROOT];
+            u64 cur = mont_pow(w, (u64)t, m);
+            const u64 step = mont_pow(w, (u64)T, m);
+            for (int k = t; k <= L / 2; k += T) {
+                put_pair(W(), k, from_mont(cur, m), P);
+                cur = mont_mul(cur, step, m);
+            }
+        });
+        ex.sync();
+        // kernel spectrum: hat = DIF(ker) / L with ker[t] = 1/t for 1 <= t <= n-1 (fast/cuckoo_fast.cu:829,838-839)
+        ex.each([&](int t, Regs<G>& rg) CF_INL {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                const int i = G::idx(0, t, j);
+                rg.x[j] = (i >= 1 && i < n) ? val(inv(), i) : 0;
+            }
+        });
+        fwd_only();
+        ex.each([&](int t, Regs<G>& rg) CF_INL {
+            const u64 linv = mi[MI_LINV];
+            const u64 linvq = shoup_companion(linv, P);
+#pragma unroll
+            for (int j = 0; j < E; ++j) put_pair(hat(), G::idx(NP - 1, t, j), canon(shoup_mul_lazy(rg.x[j], linv, linvq, P)), P);
+        });
+        ex.sync();
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Query partial sums for row q: sum_{w<q} Vs[q][w] / (M_j - w) for every query with n_j >= q
+    // (the U[w] / (M - w) sums of fast/cuckoo_fast.cu:306-323, 595-622).  The row is in the
+    // registers (layout 0, entries outside the row zero); each warp stores its own partial sum.
     // ---------------------------------------------------------------------------------------
     CF_HD void query_row(int q) {
-        u64* red = sm + Smem<G>::RED;
-        for (int jq = 0; jq < J; ++jq) {
+        for (int jq = 0; jq < kp.J; ++jq) {
             const int nj = kp.qn[jq], Mj = kp.qM[jq];
             if (nj < q) continue;
-            ex.each([&](int t, Regs<G>& rg) {
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
+                const u64* iv = inv();
                 u64 acc = 0;
-#pragma unroll
-                for (int j = 0; j < E; ++j) {
-                    const int w = G::idx(0, t, j);
-                    if (w < q) acc += sh(rg.x[j], inv, invq, Mj - w);  // < 2^63 for E <= 2^12
-                }
-                red[t] = red2(shoup_mul(acc, 1, one_q, md), P);
+                // 1/(M - w) for the slots' w (clamped to a valid entry outside the row)
+                pipe_pairs<E, PIPE_D, WIN_K>(
+                    [&](auto jc) CF_INL {
+                        const int w = G::idx(0, t, decltype(jc)::value);
+                        return iv + 2 * (w < q ? Mj - w : Mj);
+                    },
+                    [&](auto jc, u64 c, u64 cq) CF_INL {
+                        constexpr int j = decltype(jc)::value;
+                        if (G::idx(0, t, j) < q) acc += shoup_mul_lazy(rg.x[j], c, cq, P);  // < 2^57
+                    },
+                    [&](auto) CF_INL { pin(acc); });
+                const u64 part = canon(shoup_mul_lazy(acc, 1, misc()[MI_ONEQ], P));
+                ex.warp_sum_store(t, part, P, ps() + (size_t)jq * NW * (kp.n + 1) + q, (size_t)(kp.n + 1));
             });
-            const u64 s = sum_red();
-            ex.single([&]() { ps[(size_t)jq * (n + 1) + q] = s; });
         }
     }
 
     // One step of the suffix recurrence (fast/cuckoo_fast.cu:841-855).
     CF_HD void step(int v) {
-        u64* tab = sm + Smem<G>::TAB;
+        const int n = kp.n, d0 = kp.d0;
         if (v > d0) {  // stage 1: column v of S from row v of V
-            ex.each([&](int t, Regs<G>& rg) {
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
+                const u64* Vt = V();
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
                     const int i = G::idx(0, t, j);
-                    rg.x[j] = i < v ? CF_LDG(V + colV(i, n) + (v - i - 1)) : 0;
+                    // columns w < d0 of V are zero (g(w) = 0) and never written
+                    rg.x[j] = (i >= d0 && i < v) ? CF_LDG(Vt + colV(i, n) + (v - i - 1)) : 0;
                 }
             });
             query_row(v);
             convolve();
-            ex.each([&](int t, Regs<G>& rg) {
-                const u64 iv = CF_LDG(inv + v), ivq = CF_LDG(invq + v);
-                u64* col = S + colS(v, n);
-#pragma unroll
-                for (int j = 0; j < E; ++j) {
-                    const int i = G::idx(0, t, j);
-                    if (i >= v && i < n) col[i - v] = red2(shoup_mul(sh(rg.x[j], D, Dq, i - v), iv, ivq, md), P);
-                }
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
+                const u64 iv = val(inv(), v), ivq = CF_LDG(inv() + 2 * v + 1);
+                u64* col = S() + colS(v, n);
+                const u64* Dt = D();
+                pipe_pairs<E, PIPE_D, WIN_K>(
+                    [&](auto jc) CF_INL {
+                        const int i = G::idx(0, t, decltype(jc)::value);
+                        return Dt + 2 * (i >= v && i < n ? i - v : 0);
+                    },
+                    [&](auto jc, u64 c, u64 cq) CF_INL {
+                        constexpr int j = decltype(jc)::value;
+                        const int i = G::idx(0, t, j);
+                        pin(rg.x[j]);
+                        rg.x[j] = canon(shoup_mul_lazy(shoup_mul_lazy(rg.x[j], c, cq, P), iv, ivq, P));
+                        if (i >= v && i < n) col[i - v] = rg.x[j];
+                    },
+                    [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
         }
         if (v >= d0) {  // stage 2: column v of V from row v of S
-            ex.each([&](int t, Regs<G>&) {
-                power_tables(t, g_mont(v), tab);                 // g^e
-                power_tables(t, ginv_mont(v), tab + 4 * G::GT);  // g^-e
-            });
-            ex.sync();
-            ex.each([&](int t, Regs<G>& rg) {
+            ex.sync();  // column v of S is read below
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
+                const Mod m = md();
+                const u64 gi = ginv_mont(v, m);
+                u64 f = mont_pow(gi, (u64)t, m);           // g^-t
+                const u64 step = mont_pow(gi, (u64)T, m);  // g^-T
+                const u64* St = S();
+#pragma unroll
+                for (int j = 0; j < E; ++j) rg.x[j] = 0;
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
-                    const int i = G::idx(0, t, j);
-                    rg.x[j] = (i >= 1 && i <= v) ? mul_pow(CF_LDG(S + colS(i, n) + (v - i)), tab + 4 * G::GT, i) : 0;
+                    const int i = G::idx(0, t, j);  // = t + j T
+                    // columns q <= d0 of S are zero (stage 1 skipped: row q of V is zero) and never written
+                    if (i > d0 && i <= v) rg.x[j] = CF_LDG(St + colS(i, n) + (v - i));
                 }
+                window<E, WIN_K>(
+                    [&](auto jc) CF_INL {
+                        constexpr int j = decltype(jc)::value;
+                        pin(rg.x[j]);
+                        rg.x[j] = mont_mul(rg.x[j], f, m);
+                        f = mont_mul(f, step, m);
+                    },
+                    [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
             convolve();
-            ex.each([&](int t, Regs<G>& rg) {
-                const u64 dv = CF_LDG(D + v);
-                u64* col = V + colV(v, n);
-#pragma unroll
-                for (int j = 0; j < E; ++j) {
-                    const int i = G::idx(0, t, j);
-                    const int p = (i == 0) ? L : i;  // e[n] sits at index 0 when L = n
-                    if (p > v && p <= n) {
-                        const u64 pe = shoup_mul(rg.x[j], (u64)p % P, CF_LDG(Kq + p), md);
-                        u64 y = sh(dv + P2 - pe, D, Dq, p - v - 1);
-                        y = mul_pow(y, tab, p);
-                        col[p - v - 1] = red2(y, P);
-                    }
-                }
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
+                const Mod m = md();
+                const u64 gm = g_mont(v, m);
+                u64 f = mont_pow(gm, (u64)t, m);           // g^t
+                const u64 step = mont_pow(gm, (u64)T, m);  // g^T
+                const u64 dv = val(D(), v);
+                u64* col = V() + colV(v, n);
+                const u64* Dt = D();
+                const u64* Kqt = Kq();
+                const u64 fwrap = (t == 0 && n == L) ? mont_pow(gm, (u64)L, m) : 0;
+                pipe_pairs<E, PIPE_D, WIN_K>(
+                    [&](auto jc) CF_INL {
+                        const int i = G::idx(0, t, decltype(jc)::value), p = i == 0 ? L : i;
+                        return Dt + 2 * (p > v && p <= n ? p - v - 1 : 0);
+                    },
+                    [&](auto jc, u64 c, u64 cq) CF_INL {
+                        constexpr int j = decltype(jc)::value;
+                        const int i = G::idx(0, t, j);
+                        const bool wrap = (i == 0);  // e[n] sits at index 0 when L = n
+                        const int p = wrap ? L : i;
+                        pin(rg.x[j]);
+                        if (p > v && p <= n) {
+                            const u64 pe = shoup_mul_lazy(rg.x[j], (u64)p, CF_LDG(Kqt + p), P);
+                            const u64 y = shoup_mul_lazy(dv + 4 * P - pe, c, cq, P);
+                            rg.x[j] = mont_mul(y, wrap ? fwrap : f, m);
+                            col[p - v - 1] = rg.x[j];
+                        }
+                        f = mont_mul(f, step, m);
+                    },
+                    [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
         }
         ex.sync();  // column v of V is read by the next step
     }
 
-    // Horner finish (fast/cuckoo_fast.cu:877-890): N_bad = M! n! sum_k inv[k] ifact[n-k] ifact[M-k] Q^{n-k} ps[k]
+    // Horner finish (fast/cuckoo_fast.cu:877-890):
+    //   N_bad = M! n! sum_k inv[k] ifact[n-k] ifact[M-k] Q^{n-k} ps[k],  ps[k] = sum of the warp partials.
     CF_HD void finish() {
-        u64* tab = sm + Smem<G>::TAB;
+        const int n = kp.n, d0 = kp.d0;
         u64* red = sm + Smem<G>::RED;
-        // the last row n for queries with n_j = n
-        if (n > d0) {
-            ex.each([&](int t, Regs<G>& rg) {
+        if (n > d0) {  // the last row n for queries with n_j = n
+            ex.each([&](int t, Regs<G>& rg) CF_INL {
+                const u64* Vt = V();
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
                     const int i = G::idx(0, t, j);
-                    rg.x[j] = i < n ? CF_LDG(V + colV(i, n) + (n - i - 1)) : 0;
+                    rg.x[j] = (i >= d0 && i < n) ? CF_LDG(Vt + colV(i, n) + (n - i - 1)) : 0;
                 }
             });
             query_row(n);
         }
-        for (int jq = 0; jq < J; ++jq) {
+        ex.sync();
+        for (int jq = 0; jq < kp.J; ++jq) {
             const int nj = kp.qn[jq], Mj = kp.qM[jq];
-            ex.sync();
-            ex.each([&](int t, Regs<G>&) {
+            ex.each([&](int t, Regs<G>&) CF_INL {
+                const Mod m = md();
                 u64 Qm;
-                if (model == MODEL_REPLACEMENT) Qm = mont_pow(to_mont((u64)Mj, md), (u64)d, md);
-                else Qm = to_mont(red2(sh(sh(CF_LDG(fact + Mj), ifact, ifactq, d), ifact, ifactq, Mj - d), P), md);
-                power_tables(t, Qm, tab);
-            });
-            ex.sync();
-            ex.each([&](int t, Regs<G>&) {
+                if (kp.model == MODEL_REPLACEMENT) Qm = mont_pow(to_mont((u64)Mj, m), (u64)kp.d, m);
+                else Qm = to_mont(canon(sh(sh(val(fact(), Mj), ifact(), kp.d), ifact(), Mj - kp.d)), m);
+                const u64* pst = ps() + (size_t)jq * NW * (n + 1);
                 u64 acc = 0;
                 for (int k = t + 1; k <= nj; k += T) {
-                    u64 y = CF_LDG(ps + (size_t)jq * (n + 1) + k);
-                    y = sh(y, inv, invq, k);
-                    y = sh(y, ifact, ifactq, nj - k);
-                    y = sh(y, ifact, ifactq, Mj - k);
-                    y = mul_pow(y, tab, nj - k);
-                    acc = madd(acc, red2(y, P), P);
+                    u64 y = 0;
+                    for (int w = 0; w < NW; ++w) y = madd(y, pst[(size_t)w * (n + 1) + k], P);
+                    y = sh(y, inv(), k);
+                    y = sh(y, ifact(), nj - k);
+                    y = sh(y, ifact(), Mj - k);
+                    y = mont_mul(y, mont_pow(Qm, (u64)(nj - k), m), m);
+                    acc = madd(acc, y, P);
                 }
                 red[t] = acc;
             });
             const u64 s = sum_red();
-            ex.single([&]() {
-                const u64 r = red2(sh(red2(sh(s, fact, factq, nj), P), fact, factq, Mj), P);
-                kp.out[(size_t)b * J + jq] = r;
-            });
+            ex.single([&]() CF_INL { kp.out[(size_t)b * kp.J + jq] = canon(sh(canon(sh(s, fact(), nj)), fact(), Mj)); });
         }
     }
 
     CF_HD void run() {
         setup();
-        for (int v = 1; v < n; ++v) step(v);
+        for (int v = 1; v < kp.n; ++v) step(v);
         finish();
     }
 };

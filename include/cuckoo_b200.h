@@ -65,7 +65,7 @@ int cf_residues(cf_engine* e, const uint64_t* primes, int B, int nmax, int d, in
                 int J, uint64_t* residues);
 
 /* Same computation with the primes and residues in device memory, enqueued on `stream`
- * (a cudaStream_t; NULL selects the engine's own stream); returns without waiting. */
+ * (a cudaStream_t; NULL is the CUDA default stream); returns without waiting. */
 int cf_residues_async(cf_engine* e, const uint64_t* d_primes, int B, int nmax, int d, int model, const int* qn,
                       const int* qM, int J, uint64_t* d_residues, void* stream);
 

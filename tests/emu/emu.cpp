@@ -27,6 +27,11 @@ struct HostExec {
     void set_error(int* err, int code) {
         if (*err == 0) *err = code;
     }
+    // warp sums, as on the device: threads of a warp run one after another, dst starts at zero
+    void warp_sum_store(int t, u64 v, u64 P, u64* dst, size_t stride) {
+        u64* c = dst + (size_t)(t >> 5) * stride;
+        *c = madd(*c, v, P);
+    }
     void reduce_mod(u64* red, int T, u64 P) {
         u64 s = 0;
         for (int t = 0; t < T; ++t) s = madd(s, red[t], P);
@@ -59,8 +64,10 @@ extern "C" int emu_residues(const uint64_t* primes, int B, int nmax, int d, int 
     const int L = (int)cfh::transform_length((uint64_t)nmax);
     int lg = 0;
     while ((1 << lg) < L) ++lg;
-    const Layout lo = make_layout(nmax, F, L, J);
-    std::vector<u64> ws(lo.total * (size_t)B);
+    const int T = 1 << (lg - (lg >= 10 ? 5 : (lg >= 6 ? lg - 5 : 1)));
+    const Layout lo = make_layout(nmax, F, L, J, T >= 32 ? T / 32 : 1);
+    // poisoned, like reused device memory: every word the kernel reads must have been written first
+    std::vector<u64> ws(lo.total * (size_t)B, 0xA5A5A5A5A5A5A5A5ull);
     int err = 0;
     KParams kp;
     kp.primes = primes;
@@ -75,6 +82,7 @@ extern "C" int emu_residues(const uint64_t* primes, int B, int nmax, int d, int 
     kp.qM = qM;
     kp.ws = ws.data();
     kp.ws_words = lo.total;
+    kp.lay = lo;
     kp.out = out;
     kp.err = &err;
     switch (lg) {

@@ -31,18 +31,38 @@ def test_cli_output_identical_to_reference(tmp_path, name):
     assert r.stdout == golden_text(name)
 
 
-def test_cli_resume_completes_partial_file(tmp_path):
+def run_cli(binary, d, qpath, first, count, out, extra=()):
+    return subprocess.run([binary, str(d), qpath, str(first), str(count), "--out", str(out)] + list(extra),
+                          capture_output=True, text=True, check=True)
+
+
+def test_cli_resume_matches_reference_byte_for_byte(tmp_path):
+    """Resume from a file cut inside a prime's lines: the reference redoes every prime whose line
+    count is not complete (fast/cuckoo_fast.cu:697-726), so both files must evolve identically."""
+    ref_bin = os.path.join(h.ROOT, "oracle", "_ref", "cuckoo_fast_cpu")
+    if not os.path.exists(ref_bin):
+        pytest.skip("reference host build not available")
     d, queries, first, count, _ = h.load_fast_golden("fast_small_d2.txt")
+    qpath = write_queries(tmp_path, queries)
+    partial = "".join(golden_text("fast_small_d2.txt").splitlines(keepends=True)[:30])
+    mine, ref = tmp_path / "mine.txt", tmp_path / "ref.txt"
+    mine.write_text(partial)
+    ref.write_text(partial)
+    for _ in range(2):
+        run_cli(cb.CLI_PATH, d, qpath, first, count, mine, ["--batch", "7"])
+        run_cli(ref_bin, d, qpath, first, count, ref)
+        assert mine.read_text() == ref.read_text()
+    assert set(mine.read_text().splitlines()) == set(golden_text("fast_small_d2.txt").splitlines())
+
+
+def test_cli_resume_at_prime_boundary(tmp_path):
+    d, queries, first, count, lines = h.load_fast_golden("fast_small_d2.txt")
     want = golden_text("fast_small_d2.txt")
+    cut = next(k for k, ln in enumerate(lines) if ln[0] == 5)  # first line of prime 5
     out = tmp_path / "out.txt"
-    lines = want.splitlines(keepends=True)
-    # keep the first 30 lines, then cut the next prime's lines in half (an interrupted batch)
-    out.write_text("".join(lines[:30]))
-    r = subprocess.run([cb.CLI_PATH, str(d), write_queries(tmp_path, queries), str(first), str(count), "--out", str(out),
-                        "--batch", "7"], capture_output=True, text=True, check=True)
-    got = out.read_text().splitlines()
-    assert sorted(set(got)) == sorted(set(want.splitlines()))
-    # second run: nothing left to do
-    r = subprocess.run([cb.CLI_PATH, str(d), write_queries(tmp_path, queries), str(first), str(count), "--out", str(out)],
-                       capture_output=True, text=True, check=True)
+    out.write_text("".join(want.splitlines(keepends=True)[:cut]))
+    qpath = write_queries(tmp_path, queries)
+    run_cli(cb.CLI_PATH, d, qpath, first, count, out, ["--batch", "7"])
+    assert out.read_text() == want
+    r = run_cli(cb.CLI_PATH, d, qpath, first, count, out)
     assert "nothing to do" in r.stderr
