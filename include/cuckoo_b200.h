@@ -78,6 +78,26 @@ long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J);
 /* Kernel launches issued by the last cf_residues / cf_residues_async call. */
 long cf_last_launches(const cf_engine* e);
 
+/* ---- allocation-free variant (no counterpart in the reference) ---- */
+
+/* Bytes of the static device scratch used by cf_residues_noalloc (64 MiB).  One prime's table
+ * fits up to about nmax = 2800; smaller tables are batched several primes per launch. */
+#define CF_NOALLOC_SCRATCH_BYTES (64ull << 20)
+
+/* The computation of cf_residues, for callers that cannot allocate device memory (their device
+ * memory belongs to another allocator, allocation is forbidden where they run, or their device
+ * footprint must stay fixed after start-up).  No engine, no cudaMalloc/cudaFree: all scratch is
+ * a file-scope device array of CF_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until exit.  Host buffers; runs on `stream` (NULL = default stream) of the current device and
+ * returns when the residues are in `residues`.  The first call on a device resolves the array's
+ * address (make it before any stream capture).  All calls share the array, so calls that overlap
+ * on the GPU race.  Returns CF_ERR_NOMEM, without launching, when one prime's workspace exceeds
+ * the array.  No counterpart in the reference. */
+int cf_residues_noalloc(const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM, int J,
+                        uint64_t* residues, void* stream);
+/* Message for the last failed cf_residues_noalloc call ("" if none). */
+const char* cf_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
