@@ -204,7 +204,8 @@ def main():
     queries = [(n, M)]
     J = 1
     sms = torch.cuda.get_device_properties(local).multi_processor_count
-    B = a.batch or min(eng.max_batch(n, M, J), sms)
+    # one wave, one prime below what fits now: what the launch sees must still hold the whole batch
+    B = a.batch or max(1, min(eng.max_batch(n, M, J) - 1, sms))
     primes = cb.prime_range(rank * B, B)
     stream = torch.cuda.Stream()  # a dedicated stream: the events below are recorded on it
     d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")

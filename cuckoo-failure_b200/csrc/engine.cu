@@ -38,7 +38,7 @@ static KInfo kernel_for(int lg) {
         case 12: return cf_kinfo_lg12();
         case 13: return cf_kinfo_lg13();
         case 14: return cf_kinfo_lg14();
-        default: return KInfo{nullptr, 0, 0};
+        default: return KInfo{nullptr, 0, 0, 0};
     }
 }
 static constexpr int MAX_LG = 14;
@@ -85,6 +85,7 @@ static int warps_for(int lg) {
     const KInfo ki = kernel_for(lg);
     return ki.threads >= 32 ? ki.threads / 32 : 1;
 }
+static int r_for(int lg) { return kernel_for(lg).r; }
 
 static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const int* qM, int J, Plan& pl) {
     if (nmax < 1 || d < 1 || (model != CF_MODEL_SUBSET && model != CF_MODEL_REPLACEMENT) || J < 0)
@@ -104,7 +105,7 @@ static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const i
     pl.lg = lg;
     pl.F = F;
     pl.d0 = model == CF_MODEL_SUBSET ? d : 1;
-    pl.lay = make_layout(nmax, F, (int)L, J, warps_for(lg));
+    pl.lay = make_layout(nmax, F, (int)L, J, warps_for(lg), r_for(lg));
     pl.ws_words = pl.lay.total;
     return CF_OK;
 }
@@ -168,8 +169,10 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
         cap = want;
     }
     CF_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(int), s), "error reset");
-    for (int at = 0; at < B; at += (int)cap) {
-        const int nb = (int)std::min<long>(cap, B - at);
+    // equal chunks: a short tail launch would cost as much time as a full one
+    const long nchunks = (B + cap - 1) / cap, per = (B + nchunks - 1) / nchunks;
+    for (int at = 0; at < B; at += (int)per) {
+        const int nb = (int)std::min<long>(per, B - at);
         KParams kp;
         kp.primes = d_primes + at;
         kp.B = nb;
@@ -243,7 +246,7 @@ uint64_t cf_workspace_bytes(int nmax, int Mmax, int J) {
     int lg = 0;
     while ((1ull << lg) < L) ++lg;
     if (lg > MAX_LG) return 0;
-    return 8 * make_layout(nmax, F, (int)L, J, warps_for(lg)).total;
+    return 8 * make_layout(nmax, F, (int)L, J, warps_for(lg), r_for(lg)).total;
 }
 
 long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J) {

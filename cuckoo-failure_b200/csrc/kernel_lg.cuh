@@ -23,6 +23,44 @@ struct DevExec {
     }
     __device__ __forceinline__ void sync() { __syncthreads(); }
     __device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
+    // Tensor memory: one warp allocates all 512 columns for the CTA (one CTA per SM uses it);
+    // thread t of warp w owns lane 32 (w % 4) + (t % 32), columns 128 (w / 4) + [0, 128).
+    __device__ __forceinline__ void tmem_alloc(u32* slot) {
+        if ((threadIdx.x >> 5) == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             (u32)__cvta_generic_to_shared(slot)), "r"(512));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
+        tmem_sync();
+    }
+    __device__ __forceinline__ void tmem_free(u32 base) {
+        tmem_sync();
+        if ((threadIdx.x >> 5) == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(512));
+    }
+    __device__ __forceinline__ void tmem_sync() {
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    __device__ __forceinline__ static u32 tmem_addr(u32 base, int t) {
+        const int w = t >> 5;
+        return base + ((u32)(32 * (w & 3)) << 16) + (u32)(128 * (w >> 2));
+    }
+    __device__ __forceinline__ void tmem_st16(int, u32 ta, const u32 (&v)[16]) {
+        asm volatile(
+            "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(ta),
+            "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+            "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]));
+    }
+    __device__ __forceinline__ void tmem_ld16(int, u32 ta, u32 (&v)[16]) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+              "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(ta));
+    }
+    __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+    __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
     // Sum mod p of v over the calling thread's warp; lane 0 stores it at dst[warp * stride].
     __device__ __forceinline__ void warp_sum_store(int t, u64 v, u64 P, u64* dst, size_t stride) {
         const int T = (int)blockDim.x;
@@ -71,11 +109,12 @@ struct KInfo {
     kfn_t fn;
     int threads;
     size_t smem;
+    int r;  // log2 of the entries per thread
 };
 template <int LG>
 inline KInfo kinfo() {
     typedef Geo<LG, RFor<LG>::R> G;
-    return KInfo{&k_suffix<LG, RFor<LG>::R>, G::T, Smem<G>::BYTES};
+    return KInfo{&k_suffix<LG, RFor<LG>::R>, G::T, Smem<G>::BYTES, RFor<LG>::R};
 }
 
 }  // namespace cfb

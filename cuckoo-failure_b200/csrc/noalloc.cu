@@ -69,7 +69,7 @@ KInfo kernel_for(int lg) {
         case 12: return cf_kinfo_lg12();
         case 13: return cf_kinfo_lg13();
         case 14: return cf_kinfo_lg14();
-        default: return KInfo{nullptr, 0, 0};
+        default: return KInfo{nullptr, 0, 0, 0};
     }
 }
 
@@ -122,7 +122,7 @@ extern "C" int cf_residues_noalloc(const uint64_t* primes, int B, int nmax, int 
             return fail(CF_ERR_ARG, "prime " + std::to_string(p) + " is not an odd prime < 2^50 above max(n, M) with L | p-1");
     }
     if (B == 0) return CF_OK;
-    const Layout lay = make_layout(nmax, F, (int)L, J, ki.threads >= 32 ? ki.threads / 32 : 1);
+    const Layout lay = make_layout(nmax, F, (int)L, J, ki.threads >= 32 ? ki.threads / 32 : 1, ki.r);
     // scratch layout: [error word][queries: J n's then J M's as ints][primes][residues][workspaces]
     const size_t qwords = ((size_t)J + 1 + 31) & ~(size_t)31;
     const size_t fixed = HEAD_WORDS + qwords;

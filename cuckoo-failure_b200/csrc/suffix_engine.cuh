@@ -42,13 +42,40 @@ enum { MODEL_SUBSET = 0, MODEL_REPLACEMENT = 1 };
 // pairs fetched with one 16-byte load.  `ld_pair` is a volatile load and `pin` an empty volatile
 // statement that consumes a result: a load placed after a pin cannot be hoisted above the work
 // that produced the pinned value, which bounds how many constants are in flight (registers).
+//
+// L2 policy: the per-prime constant tables are re-read every step and are loaded with an
+// evict-last hint; the rows and column tiles of V and S stream through once per step and use
+// evict-first, so they do not push the tables out of L2.  V, S and the tiles are written by the
+// kernel itself, so they are read with plain coherent loads, never through the read-only path.
 #if defined(__CUDA_ARCH__)
 CF_HD void pin(u64& v) { asm volatile("" : "+l"(v)); }
 CF_HD void pin_int(int& v) { asm volatile("" : "+r"(v)); }
+CF_HD u64 policy_keep() {
+    u64 pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+CF_HD u64 policy_stream() {
+    u64 pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
 CF_HD void ld_pair(const u64* p, u64& a, u64& b) {
-    asm volatile("ld.global.nc.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
+    asm volatile("ld.global.nc.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(a), "=l"(b) : "l"(p), "l"(policy_keep()));
+}
+CF_HD u64 ld_stream(const u64* p) {
+    u64 v;
+    asm volatile("ld.global.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(policy_stream()));
+    return v;
+}
+CF_HD void st_stream(u64* p, u64 v) { asm volatile("st.global.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(p), "l"(v), "l"(policy_stream())); }
+CF_HD void ld_pair_shared(const u64* p, u64& a, u64& b) {
+    asm volatile("ld.shared.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "r"((u32)__cvta_generic_to_shared(p)));
 }
 #else
+CF_HD u64 ld_stream(const u64* p) { return *p; }
+CF_HD void st_stream(u64* p, u64 v) { *p = v; }
+CF_HD void ld_pair_shared(const u64* p, u64& a, u64& b) { a = p[0], b = p[1]; }
 CF_HD void pin(u64&) {}
 CF_HD void pin_int(int&) {}
 CF_HD void ld_pair(const u64* p, u64& a, u64& b) { a = p[0], b = p[1]; }
@@ -125,10 +152,17 @@ struct Geo {
 
 CF_HD u64 red2(u64 x, u64 m) { return x >= m ? x - m : x; }  // [0, 2m) -> [0, m)
 
+// V and S are read by rows (a step reads row v) but produced by columns (step v writes column v).
+// They are stored as packed row-major triangles, so a row read is contiguous; the columns of the
+// current TILE steps are staged column-major in VS / SS (contiguous writes) and moved into the rows
+// every TILE steps, the scheme of fast/cuckoo_fast.cu:133-144, 227-243.
+constexpr int TILE = 16;
+
 // Per-prime global workspace, in 64-bit words (every table 256-byte aligned).
 // Tables marked "pairs" hold (value, Shoup companion) interleaved: entry k at [2k], [2k+1].
 struct Layout {
-    size_t V, S, fact, ifact, inv, D, Kq, W, hat, ps, total;
+    size_t V, S, VS, SS, fact, ifact, inv, D, hat, ps, total;
+    size_t WL[8];  // pass-0 twiddles by level: WL[s] holds pairs w^(u 2^s), u = 0 .. L/2^(s+1)
 };
 CF_HD size_t lay_take(size_t& at, size_t cnt) {
     const size_t r = at;
@@ -136,24 +170,26 @@ CF_HD size_t lay_take(size_t& at, size_t cnt) {
     return r;
 }
 // nw = warps per CTA: query partial sums are kept per warp.
-CF_HD Layout make_layout(int n, int F, int L, int J, int nw) {
+CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R) {
     Layout o;
     size_t at = 0;
-    o.V = lay_take(at, (size_t)n * (n + 1) / 2);  // columns w = 0..n-1, rows p = w+1..n
-    o.S = lay_take(at, (size_t)n * (n - 1) / 2);  // columns q = 1..n-1, rows v = q..n-1
+    o.V = lay_take(at, (size_t)n * (n + 1) / 2);      // rows p = 1..n, entries w = 0..p-1
+    o.S = lay_take(at, (size_t)n * (n - 1) / 2);      // rows v = 1..n-1, entries q = 1..v
+    o.VS = lay_take(at, (size_t)TILE * (n + 1));      // column tiles, [column - v0][row]
+    o.SS = lay_take(at, (size_t)TILE * (n + 1));
     o.fact = lay_take(at, 2 * ((size_t)F + 1));   // pairs: k!
     o.ifact = lay_take(at, 2 * ((size_t)F + 1));  // pairs: 1/k!
     o.inv = lay_take(at, 2 * ((size_t)F + 1));    // pairs: 1/k
     o.D = lay_take(at, 2 * ((size_t)n + 1));      // pairs: 1/k!^2
-    o.Kq = lay_take(at, (size_t)n + 1);           // companions of the integers k
-    o.W = lay_take(at, 2 * ((size_t)L / 2 + 1));  // pairs: w^k, w of order L
+    for (int l = 0; l < 8; ++l) o.WL[l] = l < R ? lay_take(at, 2 * (((size_t)L >> (l + 1)) + 1)) : 0;  // pairs
     o.hat = lay_take(at, 2 * (size_t)L);          // pairs: spectrum of the kernel 1/t, times 1/L
     o.ps = lay_take(at, (size_t)J * nw * (n + 1));  // [J][nw][n+1]
     o.total = at;
     return o;
 }
-CF_HD size_t colV(size_t w, size_t n) { return w * n - w * (w - 1) / 2; }        // V[p][w] at colV(w) + p-w-1
-CF_HD size_t colS(size_t q, size_t n) { return (q - 1) * n - (q - 1) * q / 2; }  // S[v][q] at colS(q) + v-q
+CF_HD size_t offV(size_t p) { return p * (p - 1) / 2; }  // V[p][w] at offV(p) + w
+CF_HD size_t offS(size_t v) { return v * (v - 1) / 2; }  // S[v][q] at offS(v) + q - 1
+CF_HD int tile_v0(int v) { return 1 + TILE * ((v - 1) / TILE); }  // first column of v's tile
 
 // Launch parameters shared by all CTAs of a batch (one CTA per prime).
 struct KParams {
@@ -177,10 +213,12 @@ struct Smem {
     static constexpr int X = 0;                       // [L] transform exchange (swizzled)
     static constexpr int RED = G::L;                  // [2T + 64] reduction and scan scratch
     static constexpr int MISC = RED + 2 * G::T + 64;  // [16] modulus constants and scalars
-    static constexpr int WORDS = MISC + 16;
+    static constexpr int TWS = MISC + 16;             // pairs w^(k 2^R), k = 0 .. L/2^(R+1): passes >= 1
+    static constexpr int TWS_N = (G::L >> (G::R + 1)) + 1;
+    static constexpr int WORDS = TWS + 2 * TWS_N;
     static constexpr size_t BYTES = (size_t)WORDS * 8;
 };
-enum { MI_P = 0, MI_PINV = 1, MI_R1 = 2, MI_R2 = 3, MI_ONEQ = 4, MI_ROOT = 5, MI_LINV = 6 };
+enum { MI_P = 0, MI_PINV = 1, MI_R1 = 2, MI_R2 = 3, MI_ONEQ = 4, MI_ROOT = 5, MI_LINV = 6, MI_TMEM = 7 };
 
 template <class G>
 struct Regs {
@@ -190,6 +228,9 @@ struct Regs {
 template <class G, class X>
 struct PrimeRun {
     static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP, NW = G::NW;
+    // L = 2^14 (512 threads x 32 entries): the kernel spectrum lives in tensor memory, each thread's
+    // 32 (value, companion) pairs in its own 128 columns; smaller transforms read it from global.
+    static constexpr bool TM = (T == 512 && E == 32);
     X& ex;
     const KParams& kp;
     int b;      // prime index within the batch
@@ -204,12 +245,14 @@ struct PrimeRun {
     // workspace tables (offsets live in the kernel parameters, so these hold no registers)
     CF_HD u64* V() const { return base + kp.lay.V; }
     CF_HD u64* S() const { return base + kp.lay.S; }
+    CF_HD u64* VS() const { return base + kp.lay.VS; }
+    CF_HD u64* SS() const { return base + kp.lay.SS; }
     CF_HD u64* fact() const { return base + kp.lay.fact; }
     CF_HD u64* ifact() const { return base + kp.lay.ifact; }
     CF_HD u64* inv() const { return base + kp.lay.inv; }
     CF_HD u64* D() const { return base + kp.lay.D; }
-    CF_HD u64* Kq() const { return base + kp.lay.Kq; }
-    CF_HD u64* W() const { return base + kp.lay.W; }
+    CF_HD u64* WL(int l) const { return base + kp.lay.WL[l]; }
+    CF_HD u64* tws() const { return sm + Smem<G>::TWS; }
     CF_HD u64* hat() const { return base + kp.lay.hat; }
     CF_HD u64* ps() const { return base + kp.lay.ps; }
     CF_HD u64* misc() const { return sm + Smem<G>::MISC; }
@@ -267,12 +310,20 @@ struct PrimeRun {
     };
     // pair address of the twiddle of group F (forward: w_{2h}^j; inverse: W[L/2 - j L/2h], whose
     // negation is w_{2h}^{-j})
+    // Pass 0 reads its level's table in global memory (a warp's lanes take consecutive pairs);
+    // later passes only need multiples of 2^R, kept in shared memory.
     template <int PASS, bool FWD, int F>
     CF_HD const u64* tw_addr(int off) const {
         typedef Plan<PASS, FWD> PL;
-        constexpr int mm = PL::gm(F), ul = PL::gul(F);
-        const int j = (off + (ul << PL::bb)) << (G::LG - 1 - PL::bb - mm);
-        return W() + 2 * (FWD ? j : L / 2 - j);
+        constexpr int mm = PL::gm(F), ul = PL::gul(F), sh = G::LG - 1 - PL::bb - mm;
+        const int u = off + (ul << PL::bb);  // twiddle w^(u 2^sh)
+        if constexpr (PASS == 0) return WL(sh) + 2 * (FWD ? u : (L >> (sh + 1)) - u);
+        else return tws() + 2 * ((FWD ? u << sh : L / 2 - (u << sh)) >> G::R);
+    }
+    template <int PASS>
+    CF_HD static void ld_tw(const u64* p, u64& a, u64& b) {
+        if constexpr (PASS == 0) ld_pair(p, a, b);
+        else ld_pair_shared(p, a, b);
     }
     template <int PASS, bool FWD>
     CF_HD void pass(int t, u64 (&x)[E]) const {
@@ -283,13 +334,13 @@ struct PrimeRun {
         u64 rw[D + 1], rq[D + 1];
         window<D, 0>([&](auto fc) CF_INL {
             constexpr int f = decltype(fc)::value;
-            if constexpr (f < PL::NG && !PL::trivial_grp(f)) ld_pair(tw_addr<PASS, FWD, f>(off), rw[f], rq[f]);
+            if constexpr (f < PL::NG && !PL::trivial_grp(f)) ld_tw<PASS>(tw_addr<PASS, FWD, f>(off), rw[f], rq[f]);
         }, [&](auto) CF_INL {});
         window<PL::NB, WIN_K>(
             [&](auto qc) CF_INL {
                 constexpr int q = decltype(qc)::value, f = PL::grp(q), fn = f + D;
                 if constexpr (PL::kk(q) == 0 && fn < PL::NG && !PL::trivial_grp(fn))
-                    ld_pair(tw_addr<PASS, FWD, fn>(off), rw[fn % (D + 1)], rq[fn % (D + 1)]);
+                    ld_tw<PASS>(tw_addr<PASS, FWD, fn>(off), rw[fn % (D + 1)], rq[fn % (D + 1)]);
                 constexpr int j0 = PL::j0(q), j1 = PL::j1(q);
                 constexpr bool trivial = PL::trivial_grp(f);
                 pin(x[j0]);
@@ -359,7 +410,31 @@ struct PrimeRun {
         });
         if constexpr (PASS > 0) inv_chain<PASS - 1>();
     }
+    // spectrum pairs of chunk C (entries 4C .. 4C+3) from tensor memory, then the next chunk
+    template <int C>
+    CF_HD void tm_pointwise(int t, u32 ta, u64 (&x)[E], u32 (&b0)[16], u32 (&b1)[16]) const {
+        if constexpr (C < E / 4) {
+            u32(&cur)[16] = (C & 1) ? b1 : b0;
+            u32(&nxt)[16] = (C & 1) ? b0 : b1;
+            if constexpr (C + 1 < E / 4) ex.tmem_ld16(t, ta + 16 * (C + 1), nxt);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const u64 w = (u64)cur[4 * k] | ((u64)cur[4 * k + 1] << 32), wq = (u64)cur[4 * k + 2] | ((u64)cur[4 * k + 3] << 32);
+                x[4 * C + k] = shoup_mul_lazy(x[4 * C + k], w, wq, P);
+            }
+            ex.tmem_wait_ld();
+            tm_pointwise<C + 1>(t, ta, x, b0, b1);
+        }
+    }
     CF_HD void pointwise(int t, u64 (&x)[E]) const {
+        if constexpr (TM) {
+            const u32 ta = X::tmem_addr((u32)misc()[MI_TMEM], t);
+            u32 b0[16], b1[16];
+            ex.tmem_ld16(t, ta, b0);
+            ex.tmem_wait_ld();
+            tm_pointwise<0>(t, ta, x, b0, b1);
+            return;
+        }
         const u64* h = hat();
         pipe_pairs<E, PIPE_D, WIN_K>(
             [&](auto jc) CF_INL { return h + 2 * G::idx(NP - 1, t, decltype(jc)::value); },
@@ -499,10 +574,7 @@ struct PrimeRun {
         // inv[k] = (k-1)!/k!, D[k] = 1/k!^2, Kq[k] = companion of k; query partial sums zeroed
         ex.each([&](int t, Regs<G>&) CF_INL {
             for (int k = t; k <= F; k += T) put_pair(inv(), k, k ? canon(sh(val(ifact(), k), fact(), k - 1)) : 0, P);
-            for (int k = t; k <= n; k += T) {
-                put_pair(D(), k, canon(sh(val(ifact(), k), ifact(), k)), P);
-                Kq()[k] = shoup_companion((u64)k, P);
-            }
+            for (int k = t; k <= n; k += T) put_pair(D(), k, canon(sh(val(ifact(), k), ifact(), k)), P);
             const size_t nps = (size_t)J * NW * (n + 1);
             for (size_t k = t; k < nps; k += T) ps()[k] = 0;
         });
@@ -529,8 +601,16 @@ struct PrimeRun {
             const u64 w = mi[MI_ROOT];
             u64 cur = mont_pow(w, (u64)t, m);
             const u64 step = mont_pow(w, (u64)T, m);
-            for (int k = t; k <= L / 2; k += T) {
-                put_pair(W(), k, from_mont(cur, m), P);
+            for (int k = t; k <= L / 2; k += T) {  // w^k into every table that holds it
+                const u64 c = from_mont(cur, m), cq = shoup_companion(c, P);
+                for (int l = 0; l < G::R && (k & ((1 << l) - 1)) == 0; ++l) {
+                    u64* d = WL(l) + 2 * (k >> l);
+                    d[0] = c, d[1] = cq;
+                }
+                if ((k & ((1 << G::R) - 1)) == 0) {
+                    u64* d = tws() + 2 * (k >> G::R);
+                    d[0] = c, d[1] = cq;
+                }
                 cur = mont_mul(cur, step, m);
             }
         });
@@ -547,8 +627,23 @@ struct PrimeRun {
         ex.each([&](int t, Regs<G>& rg) CF_INL {
             const u64 linv = mi[MI_LINV];
             const u64 linvq = shoup_companion(linv, P);
+            if constexpr (TM) {
+                const u32 ta = X::tmem_addr((u32)mi[MI_TMEM], t);
 #pragma unroll
-            for (int j = 0; j < E; ++j) put_pair(hat(), G::idx(NP - 1, t, j), canon(shoup_mul_lazy(rg.x[j], linv, linvq, P)), P);
+                for (int c = 0; c < E / 4; ++c) {
+                    u32 v[16];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const u64 h = canon(shoup_mul_lazy(rg.x[4 * c + k], linv, linvq, P)), hq = shoup_companion(h, P);
+                        v[4 * k] = lo32(h), v[4 * k + 1] = hi32(h), v[4 * k + 2] = lo32(hq), v[4 * k + 3] = hi32(hq);
+                    }
+                    ex.tmem_st16(t, ta + 16 * c, v);
+                }
+                ex.tmem_wait_st();
+            } else {
+#pragma unroll
+                for (int j = 0; j < E; ++j) put_pair(hat(), G::idx(NP - 1, t, j), canon(shoup_mul_lazy(rg.x[j], linv, linvq, P)), P);
+            }
         });
         ex.sync();
     }
@@ -587,19 +682,21 @@ struct PrimeRun {
         const int n = kp.n, d0 = kp.d0;
         if (v > d0) {  // stage 1: column v of S from row v of V
             ex.each([&](int t, Regs<G>& rg) CF_INL {
-                const u64* Vt = V();
+                const u64* row = V() + offV(v);
+                const u64* tl = VS() + v;
+                const int v0 = tile_v0(v);
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
                     const int i = G::idx(0, t, j);
                     // columns w < d0 of V are zero (g(w) = 0) and never written
-                    rg.x[j] = (i >= d0 && i < v) ? CF_LDG(Vt + colV(i, n) + (v - i - 1)) : 0;
+                    rg.x[j] = (i >= d0 && i < v) ? ld_stream(i < v0 ? row + i : tl + (size_t)(i - v0) * (n + 1)) : 0;
                 }
             });
             query_row(v);
             convolve();
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const u64 iv = val(inv(), v), ivq = CF_LDG(inv() + 2 * v + 1);
-                u64* col = S() + colS(v, n);
+                u64* col = SS() + (size_t)(v - tile_v0(v)) * (n + 1);  // S[.][v], by row
                 const u64* Dt = D();
                 pipe_pairs<E, PIPE_D, WIN_K>(
                     [&](auto jc) CF_INL {
@@ -611,7 +708,7 @@ struct PrimeRun {
                         const int i = G::idx(0, t, j);
                         pin(rg.x[j]);
                         rg.x[j] = canon(shoup_mul_lazy(shoup_mul_lazy(rg.x[j], c, cq, P), iv, ivq, P));
-                        if (i >= v && i < n) col[i - v] = rg.x[j];
+                        if (i >= v && i < n) st_stream(col + i, rg.x[j]);
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
@@ -623,14 +720,16 @@ struct PrimeRun {
                 const u64 gi = ginv_mont(v, m);
                 u64 f = mont_pow(gi, (u64)t, m);           // g^-t
                 const u64 step = mont_pow(gi, (u64)T, m);  // g^-T
-                const u64* St = S();
+                const u64* row = S() + offS(v) - 1;
+                const u64* tl = SS() + v;
+                const int v0 = tile_v0(v);
 #pragma unroll
                 for (int j = 0; j < E; ++j) rg.x[j] = 0;
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
                     const int i = G::idx(0, t, j);  // = t + j T
                     // columns q <= d0 of S are zero (stage 1 skipped: row q of V is zero) and never written
-                    if (i > d0 && i <= v) rg.x[j] = CF_LDG(St + colS(i, n) + (v - i));
+                    if (i > d0 && i <= v) rg.x[j] = ld_stream(i < v0 ? row + i : tl + (size_t)(i - v0) * (n + 1));
                 }
                 window<E, WIN_K>(
                     [&](auto jc) CF_INL {
@@ -648,9 +747,9 @@ struct PrimeRun {
                 u64 f = mont_pow(gm, (u64)t, m);           // g^t
                 const u64 step = mont_pow(gm, (u64)T, m);  // g^T
                 const u64 dv = val(D(), v);
-                u64* col = V() + colV(v, n);
+                u64* col = VS() + (size_t)(v - tile_v0(v)) * (n + 1);  // V[.][v], by row
                 const u64* Dt = D();
-                const u64* Kqt = Kq();
+                const u64 mu = misc()[MI_ONEQ];  // floor(2^64 / p)
                 const u64 fwrap = (t == 0 && n == L) ? mont_pow(gm, (u64)L, m) : 0;
                 pipe_pairs<E, PIPE_D, WIN_K>(
                     [&](auto jc) CF_INL {
@@ -664,17 +763,42 @@ struct PrimeRun {
                         const int p = wrap ? L : i;
                         pin(rg.x[j]);
                         if (p > v && p <= n) {
-                            const u64 pe = shoup_mul_lazy(rg.x[j], (u64)p, CF_LDG(Kqt + p), P);
-                            const u64 y = shoup_mul_lazy(dv + 4 * P - pe, c, cq, P);
+                            // p e[p]: with p floor(2^64/p) for the companion the quotient estimate
+                            // loses at most p (x < 8P) / 2^64 < 8 more, so pe < 12P
+                            const u64 pe = shoup_mul_lazy(rg.x[j], (u64)p, (u64)p * mu, P);
+                            const u64 y = shoup_mul_lazy(dv + 12 * P - pe, c, cq, P);
                             rg.x[j] = mont_mul(y, wrap ? fwrap : f, m);
-                            col[p - v - 1] = rg.x[j];
+                            st_stream(col + p, rg.x[j]);
                         }
                         f = mont_mul(f, step, m);
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
         }
-        ex.sync();  // column v of V is read by the next step
+        const int v0 = tile_v0(v);
+        if (v - v0 == TILE - 1 || v == n - 1) {  // move the tile's columns v0 .. v into the rows
+            ex.sync();
+            ex.each([&](int t, Regs<G>&) CF_INL {
+                const int cnt = v - v0 + 1;
+                for (int r = t; r <= n; r += T) {
+                    if (r < n) {  // row r of S: entries q = v0 .. min(v, r), written for q > d0
+                        u64* dst = S() + offS(r) - 1;
+                        const u64* srcs = SS() + r;
+                        for (int c = 0; c < cnt; ++c) {
+                            const int q = v0 + c;
+                            if (q > d0 && q <= r) st_stream(dst + q, ld_stream(srcs + (size_t)c * (n + 1)));
+                        }
+                    }
+                    u64* dst = V() + offV(r);  // row r of V: entries w = v0 .. min(v, r-1), written for w >= d0
+                    const u64* srcv = VS() + r;
+                    for (int c = 0; c < cnt; ++c) {
+                        const int w = v0 + c;
+                        if (w >= d0 && w < r) st_stream(dst + w, ld_stream(srcv + (size_t)c * (n + 1)));
+                    }
+                }
+            });
+        }
+        ex.sync();  // row v + 1 is read by the next step
     }
 
     // Horner finish (fast/cuckoo_fast.cu:877-890):
@@ -684,11 +808,11 @@ struct PrimeRun {
         u64* red = sm + Smem<G>::RED;
         if (n > d0) {  // the last row n for queries with n_j = n
             ex.each([&](int t, Regs<G>& rg) CF_INL {
-                const u64* Vt = V();
+                const u64* row = V() + offV(n);  // every column is in the rows after the last flush
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
                     const int i = G::idx(0, t, j);
-                    rg.x[j] = (i >= d0 && i < n) ? CF_LDG(Vt + colV(i, n) + (n - i - 1)) : 0;
+                    rg.x[j] = (i >= d0 && i < n) ? ld_stream(row + i) : 0;
                 }
             });
             query_row(n);
@@ -720,9 +844,11 @@ struct PrimeRun {
     }
 
     CF_HD void run() {
+        if constexpr (TM) ex.tmem_alloc((u32*)(misc() + MI_TMEM));
         setup();
         for (int v = 1; v < kp.n; ++v) step(v);
         finish();
+        if constexpr (TM) ex.tmem_free((u32)misc()[MI_TMEM]);
     }
 };
 

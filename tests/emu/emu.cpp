@@ -4,6 +4,7 @@
 // It is never linked into the product library and is not a fallback for it.
 #include <cstdint>
 #include <cstring>
+#include <stdexcept>
 #include <vector>
 
 #include "../../cuckoo-failure_b200/csrc/host_common.hpp"
@@ -27,6 +28,28 @@ struct HostExec {
     void set_error(int* err, int code) {
         if (*err == 0) *err = code;
     }
+    // tensor memory: 128 lanes x 512 columns of 32-bit words, same ownership as on the device
+    std::vector<u32> tm = std::vector<u32>(128 * 512, 0xDEADBEEFu);
+    void tmem_alloc(u32* slot) { *slot = 0; }
+    void tmem_free(u32) {}
+    void tmem_sync() {}
+    static u32 tmem_addr(u32 base, int t) {
+        const int w = t >> 5;
+        return base + ((u32)(32 * (w & 3)) << 16) + (u32)(128 * (w >> 2));
+    }
+    u32* tmem_word(int t, u32 ta, int k) {
+        const int lane = (int)(ta >> 16) + (t & 31), col = (int)(ta & 0xFFFF) + k;
+        if (lane >= 128 || col >= 512) throw std::runtime_error("tensor memory address out of range");
+        return &tm[(size_t)lane * 512 + col];
+    }
+    void tmem_st16(int t, u32 ta, const u32 (&v)[16]) {
+        for (int k = 0; k < 16; ++k) *tmem_word(t, ta, k) = v[k];
+    }
+    void tmem_ld16(int t, u32 ta, u32 (&v)[16]) {
+        for (int k = 0; k < 16; ++k) v[k] = *tmem_word(t, ta, k);
+    }
+    void tmem_wait_ld() {}
+    void tmem_wait_st() {}
     // warp sums, as on the device: threads of a warp run one after another, dst starts at zero
     void warp_sum_store(int t, u64 v, u64 P, u64* dst, size_t stride) {
         u64* c = dst + (size_t)(t >> 5) * stride;
@@ -64,8 +87,8 @@ extern "C" int emu_residues(const uint64_t* primes, int B, int nmax, int d, int 
     const int L = (int)cfh::transform_length((uint64_t)nmax);
     int lg = 0;
     while ((1 << lg) < L) ++lg;
-    const int T = 1 << (lg - (lg >= 10 ? 5 : (lg >= 6 ? lg - 5 : 1)));
-    const Layout lo = make_layout(nmax, F, L, J, T >= 32 ? T / 32 : 1);
+    const int R = lg >= 10 ? 5 : (lg >= 6 ? lg - 5 : 1), T = 1 << (lg - R);
+    const Layout lo = make_layout(nmax, F, L, J, T >= 32 ? T / 32 : 1, R);
     // poisoned, like reused device memory: every word the kernel reads must have been written first
     std::vector<u64> ws(lo.total * (size_t)B, 0xA5A5A5A5A5A5A5A5ull);
     int err = 0;
