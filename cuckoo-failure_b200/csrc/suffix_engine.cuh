@@ -11,8 +11,8 @@
 //   * every multiplication by a stored constant is a Shoup product with a precomputed companion;
 //     inside the transforms values stay lazily reduced ([0, 4p) forward, [0, 8p) inverse);
 //   * the stage factors are folded into what is stored, so stage 1 needs no multiply on input:
-//       Vs[p][w] = V[p][w] / (w! (p-1-w)! (p-1)!)        (stored V, column-major)
-//       Ss[v][q] = S[v][q] / (q! (v-q)! v!)              (stored S, column-major)
+//       Vs[p][w] = V[p][w] / (w! (p-1-w)! (p-1)!)        (stored V)
+//       Ss[v][q] = S[v][q] / (q! (v-q)! v!)              (stored S)
 //     which turns the reference's stage relations into
 //       stage 1:  Ss[v'][v] = D[v'-v] inv[v] conv(Vs[v][.])[v'],            D[k] = 1/k!^2
 //       stage 2:  Vs[p][v]  = g^p D[p-v-1] (D[v] - p conv(Ss[v][q] g^-q)[p])
@@ -153,10 +153,39 @@ struct Geo {
 CF_HD u64 red2(u64 x, u64 m) { return x >= m ? x - m : x; }  // [0, 2m) -> [0, m)
 
 // V and S are read by rows (a step reads row v) but produced by columns (step v writes column v).
-// They are stored as packed row-major triangles, so a row read is contiguous; the columns of the
-// current TILE steps are staged column-major in VS / SS (contiguous writes) and moved into the rows
-// every TILE steps, the scheme of fast/cuckoo_fast.cu:133-144, 227-243.
+// The columns of the current TILE steps are staged column-major in VS / SS (contiguous writes) and
+// moved into row storage every TILE steps, the scheme of fast/cuckoo_fast.cu:133-144, 227-243.
+//
+// Row storage is made of TILE x TILE blocks: block (P, W) holds rows 1 + 16P .. 16 + 16P and
+// columns 1 + 16W .. 16 + 16W, row-major (a row's 16 entries are one 128-byte line).  Only blocks
+// below the diagonal (W < P) are stored; a row's own group of columns is read from the staging
+// tile.  Block (P, W) is written when tile W is flushed and dead once the steps of tile P have read
+// its rows (row n of V stays until the finish), so at most (k + 1)(G - 1 - k) blocks are live
+// after flush k, G = number of row groups.  The blocks map onto an (G - h) x h array of cells,
+// h = ceil(G / 2), that is exactly that peak:
+//   W < h <= P : cell (P - h, W)          the rectangle, live through the middle of the run
+//   P < h      : cell (W, P)              rows read before step 16h; their cell's rectangle block
+//                                        is written at flush P, after its last read
+//   h <= W     : cell (W - h, P - h - 1)  written from flush h on, into cells whose rectangle
+//                                        block was read in tile W, before that flush
+// so a prime's V and S take about n^2 / 4 words each instead of n^2 / 2 for packed triangles.
 constexpr int TILE = 16;
+CF_HD int grp(int x) { return (x - 1) >> 4; }  // row / column group of index x >= 1
+CF_HD int block_h(int n) { return (((n - 1) >> 4) + 2) >> 1; }  // h = ceil(G / 2), G = grp(n) + 1
+CF_HD size_t block_count(int n) {
+    if (n < 1) return 0;
+    const size_t G = (size_t)grp(n) + 1, h = (size_t)block_h(n);
+    return (G - h) * h;
+}
+CF_HD size_t block_cell(int P, int W, int h) {  // W < P
+    if (P < h) return (size_t)W * h + P;
+    if (W < h) return (size_t)(P - h) * h + W;
+    return (size_t)(W - h) * h + (P - h - 1);
+}
+// word offset of entry (row r, column c), grp(c) < grp(r), inside a block pool
+CF_HD size_t blk_off(int r, int c, int h) {
+    return (block_cell(grp(r), grp(c), h) << 8) + ((size_t)((r - 1) & 15) << 4) + (size_t)((c - 1) & 15);
+}
 
 // Per-prime global workspace, in 64-bit words (every table 256-byte aligned).
 // Tables marked "pairs" hold (value, Shoup companion) interleaved: entry k at [2k], [2k+1].
@@ -173,8 +202,8 @@ CF_HD size_t lay_take(size_t& at, size_t cnt) {
 CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R) {
     Layout o;
     size_t at = 0;
-    o.V = lay_take(at, (size_t)n * (n + 1) / 2);      // rows p = 1..n, entries w = 0..p-1
-    o.S = lay_take(at, (size_t)n * (n - 1) / 2);      // rows v = 1..n-1, entries q = 1..v
+    o.V = lay_take(at, block_count(n) << 8);         // rows p = 1..n, entries w = 1..p-1 (blocks)
+    o.S = lay_take(at, block_count(n) << 8);         // rows v = 1..n-1, entries q = 1..v (blocks)
     o.VS = lay_take(at, (size_t)TILE * (n + 1));      // column tiles, [column - v0][row]
     o.SS = lay_take(at, (size_t)TILE * (n + 1));
     o.fact = lay_take(at, 2 * ((size_t)F + 1));   // pairs: k!
@@ -187,8 +216,6 @@ CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R) {
     o.total = at;
     return o;
 }
-CF_HD size_t offV(size_t p) { return p * (p - 1) / 2; }  // V[p][w] at offV(p) + w
-CF_HD size_t offS(size_t v) { return v * (v - 1) / 2; }  // S[v][q] at offS(v) + q - 1
 CF_HD int tile_v0(int v) { return 1 + TILE * ((v - 1) / TILE); }  // first column of v's tile
 
 // Launch parameters shared by all CTAs of a batch (one CTA per prime).
@@ -648,6 +675,19 @@ struct PrimeRun {
         ex.sync();
     }
 
+    // Row r of V or S into the registers (layout 0): the slot of index i gets entry i of the row
+    // for lo <= i < hi, zero elsewhere.  Columns of earlier groups come from the blocks, those of
+    // r's own group from the staging tile.
+    CF_HD void load_row(int t, u64 (&x)[E], const u64* pool, const u64* tile, int r, int lo, int hi) const {
+        const int n = kp.n, v0 = tile_v0(r), h = block_h(n);
+        const u64* tl = tile + r;
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+            const int i = G::idx(0, t, j);
+            x[j] = (i >= lo && i < hi) ? ld_stream(i < v0 ? pool + blk_off(r, i, h) : tl + (size_t)(i - v0) * (n + 1)) : 0;
+        }
+    }
+
     // ---------------------------------------------------------------------------------------
     // Query partial sums for row q: sum_{w<q} Vs[q][w] / (M_j - w) for every query with n_j >= q
     // (the U[w] / (M - w) sums of fast/cuckoo_fast.cu:306-323, 595-622).  The row is in the
@@ -682,15 +722,7 @@ struct PrimeRun {
         const int n = kp.n, d0 = kp.d0;
         if (v > d0) {  // stage 1: column v of S from row v of V
             ex.each([&](int t, Regs<G>& rg) CF_INL {
-                const u64* row = V() + offV(v);
-                const u64* tl = VS() + v;
-                const int v0 = tile_v0(v);
-#pragma unroll
-                for (int j = 0; j < E; ++j) {
-                    const int i = G::idx(0, t, j);
-                    // columns w < d0 of V are zero (g(w) = 0) and never written
-                    rg.x[j] = (i >= d0 && i < v) ? ld_stream(i < v0 ? row + i : tl + (size_t)(i - v0) * (n + 1)) : 0;
-                }
+                load_row(t, rg.x, V(), VS(), v, d0, v);  // columns w < d0 of V are zero (g(w) = 0), never written
             });
             query_row(v);
             convolve();
@@ -720,17 +752,8 @@ struct PrimeRun {
                 const u64 gi = ginv_mont(v, m);
                 u64 f = mont_pow(gi, (u64)t, m);           // g^-t
                 const u64 step = mont_pow(gi, (u64)T, m);  // g^-T
-                const u64* row = S() + offS(v) - 1;
-                const u64* tl = SS() + v;
-                const int v0 = tile_v0(v);
-#pragma unroll
-                for (int j = 0; j < E; ++j) rg.x[j] = 0;
-#pragma unroll
-                for (int j = 0; j < E; ++j) {
-                    const int i = G::idx(0, t, j);  // = t + j T
-                    // columns q <= d0 of S are zero (stage 1 skipped: row q of V is zero) and never written
-                    if (i > d0 && i <= v) rg.x[j] = ld_stream(i < v0 ? row + i : tl + (size_t)(i - v0) * (n + 1));
-                }
+                // columns q <= d0 of S are zero (stage 1 skipped: row q of V is zero), never written
+                load_row(t, rg.x, S(), SS(), v, d0 + 1, v + 1);
                 window<E, WIN_K>(
                     [&](auto jc) CF_INL {
                         constexpr int j = decltype(jc)::value;
@@ -778,23 +801,21 @@ struct PrimeRun {
         const int v0 = tile_v0(v);
         if (v - v0 == TILE - 1 || v == n - 1) {  // move the tile's columns v0 .. v into the rows
             ex.sync();
+            // rows of later groups only: a row of this tile's group reads these columns from the tile
             ex.each([&](int t, Regs<G>&) CF_INL {
-                const int cnt = v - v0 + 1;
-                for (int r = t; r <= n; r += T) {
-                    if (r < n) {  // row r of S: entries q = v0 .. min(v, r), written for q > d0
-                        u64* dst = S() + offS(r) - 1;
+                const int cnt = v - v0 + 1, h = block_h(n);
+                for (int r = v0 + TILE + t; r <= n; r += T) {
+                    const size_t off = blk_off(r, v0, h);  // columns v0 + c at off + c
+                    if (r < n) {  // row r of S: entries q = v0 .. v, written for q > d0
+                        u64* dst = S() + off;
                         const u64* srcs = SS() + r;
-                        for (int c = 0; c < cnt; ++c) {
-                            const int q = v0 + c;
-                            if (q > d0 && q <= r) st_stream(dst + q, ld_stream(srcs + (size_t)c * (n + 1)));
-                        }
+                        for (int c = 0; c < cnt; ++c)
+                            if (v0 + c > d0) st_stream(dst + c, ld_stream(srcs + (size_t)c * (n + 1)));
                     }
-                    u64* dst = V() + offV(r);  // row r of V: entries w = v0 .. min(v, r-1), written for w >= d0
+                    u64* dst = V() + off;  // row r of V: entries w = v0 .. v, written for w >= d0
                     const u64* srcv = VS() + r;
-                    for (int c = 0; c < cnt; ++c) {
-                        const int w = v0 + c;
-                        if (w >= d0 && w < r) st_stream(dst + w, ld_stream(srcv + (size_t)c * (n + 1)));
-                    }
+                    for (int c = 0; c < cnt; ++c)
+                        if (v0 + c >= d0) st_stream(dst + c, ld_stream(srcv + (size_t)c * (n + 1)));
                 }
             });
         }
@@ -807,14 +828,7 @@ struct PrimeRun {
         const int n = kp.n, d0 = kp.d0;
         u64* red = sm + Smem<G>::RED;
         if (n > d0) {  // the last row n for queries with n_j = n
-            ex.each([&](int t, Regs<G>& rg) CF_INL {
-                const u64* row = V() + offV(n);  // every column is in the rows after the last flush
-#pragma unroll
-                for (int j = 0; j < E; ++j) {
-                    const int i = G::idx(0, t, j);
-                    rg.x[j] = (i >= d0 && i < n) ? ld_stream(row + i) : 0;
-                }
-            });
+            ex.each([&](int t, Regs<G>& rg) CF_INL { load_row(t, rg.x, V(), VS(), n, d0, n); });
             query_row(n);
         }
         ex.sync();

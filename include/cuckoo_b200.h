@@ -81,7 +81,7 @@ long cf_last_launches(const cf_engine* e);
 /* ---- allocation-free variant (no counterpart in the reference) ---- */
 
 /* Bytes of the static device scratch used by cf_residues_noalloc (64 MiB).  One prime's table
- * fits up to about nmax = 2800; smaller tables are batched several primes per launch. */
+ * fits up to about nmax = 4000; smaller tables are batched several primes per launch. */
 #define CF_NOALLOC_SCRATCH_BYTES (64ull << 20)
 
 /* The computation of cf_residues, for callers that cannot allocate device memory (their device
