@@ -69,12 +69,18 @@ CF_HD u64 ld_stream(const u64* p) {
     return v;
 }
 CF_HD void st_stream(u64* p, u64 v) { asm volatile("st.global.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(p), "l"(v), "l"(policy_stream())); }
+// one full 32-byte sector (p 32-byte aligned)
+CF_HD void st_stream4(u64* p, u64 a, u64 b, u64 c, u64 d) {
+    asm volatile("st.global.L2::cache_hint.v4.u64 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "l"(a), "l"(b), "l"(c), "l"(d),
+                 "l"(policy_stream()));
+}
 CF_HD void ld_pair_shared(const u64* p, u64& a, u64& b) {
     asm volatile("ld.shared.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "r"((u32)__cvta_generic_to_shared(p)));
 }
 #else
 CF_HD u64 ld_stream(const u64* p) { return *p; }
 CF_HD void st_stream(u64* p, u64 v) { *p = v; }
+CF_HD void st_stream4(u64* p, u64 a, u64 b, u64 c, u64 d) { p[0] = a, p[1] = b, p[2] = c, p[3] = d; }
 CF_HD void ld_pair_shared(const u64* p, u64& a, u64& b) { a = p[0], b = p[1]; }
 CF_HD void pin(u64&) {}
 CF_HD void pin_int(int&) {}
@@ -801,21 +807,37 @@ struct PrimeRun {
         const int v0 = tile_v0(v);
         if (v - v0 == TILE - 1 || v == n - 1) {  // move the tile's columns v0 .. v into the rows
             ex.sync();
-            // rows of later groups only: a row of this tile's group reads these columns from the tile
+            // Rows of later groups only: a row of this tile's group reads these columns from the tile.
+            // A full tile goes out in whole 32-byte sectors (4 columns of a block row).
             ex.each([&](int t, Regs<G>&) CF_INL {
                 const int cnt = v - v0 + 1, h = block_h(n);
+                const size_t cs = (size_t)n + 1;  // tile column stride
                 for (int r = v0 + TILE + t; r <= n; r += T) {
                     const size_t off = blk_off(r, v0, h);  // columns v0 + c at off + c
                     if (r < n) {  // row r of S: entries q = v0 .. v, written for q > d0
                         u64* dst = S() + off;
-                        const u64* srcs = SS() + r;
-                        for (int c = 0; c < cnt; ++c)
-                            if (v0 + c > d0) st_stream(dst + c, ld_stream(srcs + (size_t)c * (n + 1)));
+                        const u64* src = SS() + r;
+                        if (cnt == TILE && v0 > d0) {
+#pragma unroll
+                            for (int c = 0; c < TILE; c += 4)
+                                st_stream4(dst + c, ld_stream(src + c * cs), ld_stream(src + (c + 1) * cs),
+                                           ld_stream(src + (c + 2) * cs), ld_stream(src + (c + 3) * cs));
+                        } else {
+                            for (int c = 0; c < cnt; ++c)
+                                if (v0 + c > d0) st_stream(dst + c, ld_stream(src + c * cs));
+                        }
                     }
                     u64* dst = V() + off;  // row r of V: entries w = v0 .. v, written for w >= d0
-                    const u64* srcv = VS() + r;
-                    for (int c = 0; c < cnt; ++c)
-                        if (v0 + c >= d0) st_stream(dst + c, ld_stream(srcv + (size_t)c * (n + 1)));
+                    const u64* src = VS() + r;
+                    if (cnt == TILE && v0 >= d0) {
+#pragma unroll
+                        for (int c = 0; c < TILE; c += 4)
+                            st_stream4(dst + c, ld_stream(src + c * cs), ld_stream(src + (c + 1) * cs),
+                                       ld_stream(src + (c + 2) * cs), ld_stream(src + (c + 3) * cs));
+                    } else {
+                        for (int c = 0; c < cnt; ++c)
+                            if (v0 + c >= d0) st_stream(dst + c, ld_stream(src + c * cs));
+                    }
                 }
             });
         }
