@@ -27,13 +27,16 @@ def write_queries(tmp_path, queries):
 def test_cli_output_identical_to_reference(tmp_path, name):
     d, queries, first, count, _ = h.load_fast_golden(name)
     r = subprocess.run([cb.CLI_PATH, str(d), write_queries(tmp_path, queries), str(first), str(count)],
-                       capture_output=True, text=True, check=True)
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
     assert r.stdout == golden_text(name)
 
 
 def run_cli(binary, d, qpath, first, count, out, extra=()):
-    return subprocess.run([binary, str(d), qpath, str(first), str(count), "--out", str(out)] + list(extra),
-                          capture_output=True, text=True, check=True)
+    r = subprocess.run([binary, str(d), qpath, str(first), str(count), "--out", str(out)] + list(extra),
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return r
 
 
 def test_cli_resume_matches_reference_byte_for_byte(tmp_path):
