@@ -1,6 +1,6 @@
 // cuckoo_fast_b200: the host driver of the reference's batch engine (fast/cuckoo_fast.cu:648-904)
 // with the GPU behind the C ABI of include/cuckoo_b200.h.  Same command line, same resume rules,
-// same output lines, so fast/post_gmp.py (or this package's crt.py) combines the residues as before.
+// same output lines, so fast/post_gmp.py (or this package's crt.py, which needs no gmpy2) combines the residues as before.
 //
 //   cuckoo_fast_b200 D QUERIES FIRST COUNT [--batch B] [--out FILE] [--device N] [--replacement]
 //
