@@ -205,6 +205,13 @@ long cf_prime_range(long first, long count, uint64_t* out) {
     return (long)v.size();
 }
 long cf_need(int n, int M, int d, int model) { return cfh::need(n, M, d, model); }
+long cf_lib_primes(int n, int M, int d, int model, uint64_t* out, long cap) {
+    if (n < 1 || M < 1 || d < 1 || (model == CF_MODEL_SUBSET && d > M) || cap < 0 || (cap > 0 && !out)) return -1;
+    const std::vector<u64> v = cfh::lib_primes_for(n, M, d, model);
+    if (v.empty()) return -1;
+    std::copy(v.begin(), v.begin() + std::min<long>(cap, (long)v.size()), out);
+    return (long)v.size();
+}
 uint64_t cf_transform_length(uint64_t nmax) { return cfh::transform_length(nmax); }
 
 int cf_engine_create(int device, cf_engine** out) {

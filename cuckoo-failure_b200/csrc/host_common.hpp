@@ -1,6 +1,7 @@
 // Host-side helpers with the reference's exact semantics (fast/cuckoo_fast.cu:391-472): the
 // fixed prime list, the prime count need(), the transform length.  Shared by the C ABI and the CLI.
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -74,6 +75,52 @@ inline u64 transform_length(u64 nmax) {
     u64 L = 1;
     while (L < nmax) L <<= 1;
     return L < 16 ? 16 : L;
+}
+
+// ---- the 32-bit library's prime choice (src/cuckoo_fail.cpp:151-170) ----
+
+// `count` primes p = c 2^k + 1 < 2^32 with c odd (so 2^k exactly divides p - 1), k from 31 down to
+// min_pow2, c from its largest value down; returned largest first
+// (include/cuckoo/modint.hpp:183-196).  Empty if there are not that many.
+inline std::vector<u64> lib_ntt_primes(int count, int min_pow2) {
+    std::vector<u64> out;
+    for (int k = 31; k >= min_pow2 && (int)out.size() < count; --k) {
+        long long c = (long long)((((1ull << 32) - 2)) >> k);
+        if (c % 2 == 0) --c;
+        for (; c >= 1 && (int)out.size() < count; c -= 2) {
+            const u64 p = ((u64)c << k) + 1;
+            if (is_prime(p)) out.push_back(p);
+        }
+    }
+    if ((int)out.size() < count) return {};
+    std::sort(out.rbegin(), out.rend());
+    return out;
+}
+
+// The primes `cuckoo_fail single -n n -M M -d d` reconstructs N_bad from: the fewest primes of the
+// list above whose product exceeds 4 Q^n, grown from n log2 Q / 31 + 2 as the library does, with
+// its long-double sums.  The transform length there is max(2, next_pow2(n))
+// (include/cuckoo/single_table.hpp:175).
+inline std::vector<u64> lib_primes_for(int n, int M, int d, int model) {
+    long double lq = 0;
+    if (model == 1) lq = d * std::log2((long double)M);
+    else
+        for (int i = 0; i < d; ++i) lq += std::log2((long double)(M - i)) - std::log2((long double)(i + 1));
+    const long double bits = n * lq;
+    u64 L = 1;
+    while (L < (u64)n) L <<= 1;
+    if (L < 2) L = 2;
+    int min_pow2 = 0;
+    while ((1ull << min_pow2) < L) ++min_pow2;
+    int count = (int)(bits / 31) + 2;
+    while (true) {
+        std::vector<u64> ps = lib_ntt_primes(count, min_pow2);
+        if (ps.empty()) return ps;
+        long double have = 0;
+        for (u64 p : ps) have += std::log2((long double)p);
+        if (have > bits + 2) return ps;
+        count += (int)((bits + 2 - have) / 31) + 1;
+    }
 }
 
 }  // namespace cfh

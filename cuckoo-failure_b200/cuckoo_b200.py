@@ -47,6 +47,8 @@ def lib():
         L.cf_prime_range.restype = ctypes.c_long
         L.cf_need.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.cf_need.restype = ctypes.c_long
+        L.cf_lib_primes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u64p, ctypes.c_long]
+        L.cf_lib_primes.restype = ctypes.c_long
         L.cf_transform_length.argtypes = [ctypes.c_uint64]
         L.cf_transform_length.restype = ctypes.c_uint64
         L.cf_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
@@ -83,6 +85,16 @@ def need(n, M, d, model=MODEL_SUBSET):
 
 def transform_length(nmax):
     return int(lib().cf_transform_length(nmax))
+
+
+def lib_primes(n, M, d, model=MODEL_SUBSET):
+    """The 32-bit primes of the library CLI for (n, M, d) (src/cuckoo_fail.cpp:151-170)."""
+    k = int(lib().cf_lib_primes(n, M, d, model, None, 0))
+    if k < 0:
+        raise ValueError(f"no prime set for n={n}, M={M}, d={d}")
+    out = np.zeros(k, dtype=np.uint64)
+    lib().cf_lib_primes(n, M, d, model, out.ctypes.data_as(_u64p), k)
+    return [int(x) for x in out]
 
 
 def workspace_bytes(nmax, Mmax, J):

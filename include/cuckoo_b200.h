@@ -45,6 +45,13 @@ long cf_need(int n, int M, int d, int model);
 /* max(16, next_pow2(nmax)).  Replaces transform_length, fast/cuckoo_fast.cu:460-472. */
 uint64_t cf_transform_length(uint64_t nmax);
 
+/* The 32-bit NTT primes the library CLI (`cuckoo_fail single -n n -M M -d d [--replacement]`)
+ * reconstructs N_bad from, largest first: replaces ntt_primes and the prime-count loop,
+ * include/cuckoo/modint.hpp:183-196 and src/cuckoo_fail.cpp:151-170.  Every one is usable by
+ * cf_residues for a table of nmax = n.  Returns how many there are (writing at most `cap`), or
+ * -1 on bad arguments. */
+long cf_lib_primes(int n, int M, int d, int model, uint64_t* out, long cap);
+
 /* ---- engine ---- */
 
 /* Bind a CUDA device and create the engine's stream.  Replaces the CUDA back end's implicit
