@@ -79,6 +79,11 @@ static int run_lg(const KParams& kp) {
     return 0;
 }
 
+// The engine's block map of V / S row storage (suffix_engine.cuh), for the lifetime test.
+extern "C" long emu_block_cell(int P, int W, int h) { return (long)block_cell(P, W, h); }
+extern "C" long emu_block_count(int n) { return (long)block_count(n); }
+extern "C" int emu_block_h(int n) { return block_h(n); }
+
 extern "C" int emu_residues(const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM, int J,
                             uint64_t* out) {
     int F = nmax;
