@@ -142,6 +142,44 @@ def golden_check(n, M, d):
     return out
 
 
+def serving_run(device, seconds, rate=200.0, n_lo=64, n_hi=2048, budget_gb=150.0, plain_sample=16):
+    """Served-query latency: a seeded Poisson stream (rate per second, n log-uniform in [n_lo, n_hi],
+    M = n U[1.5, 4], d in {2, 3, 4}) through serve.py's continuous-batching loop over resident
+    tables built before the clock starts for (n_hi, 4 n_hi, d); beside it the plain form, the same
+    requests each rebuilt alone (cf_residues over its primes, then CRT), on a sample."""
+    import numpy as np
+
+    import crt
+    import cuckoo_b200 as cb
+    import serve
+
+    stream = serve.poisson_stream(seconds, rate, n_lo, n_hi, seed=20261203)
+    with cb.Engine(device) as eng:
+        t0 = time.perf_counter()
+        warm = [(n_hi, 4 * n_hi, dd) for dd in (2, 3, 4)]
+        srv_lat, _, stats = serve.run(stream, eng, budget_gb * 1e9, warm=warm)
+        total = time.perf_counter() - t0
+        plain = []
+        for _, n, M, dd in stream[:: max(1, len(stream) // plain_sample)][:plain_sample]:
+            s0 = time.perf_counter()
+            ps = cb.prime_range(0, cb.need(n, M, dd))
+            r = eng.residues(ps, n, dd, [(n, M)])
+            crt.crt(list(zip(ps, (int(v) for v in r[:, 0]))))
+            plain.append(time.perf_counter() - s0)
+    pr = serve.percentiles(srv_lat)
+    return {"workload": f"Poisson {rate:g} req/s for {seconds:g} s, n log-uniform [{n_lo}, {n_hi}], M/n U[1.5, 4], "
+                        f"d in {{2,3,4}}; tables resident (warm) under a {budget_gb:g} GB budget",
+            "p50_ms": pr.get("p50_ms"), "p99_ms": pr.get("p99_ms"), "max_ms": pr.get("max_ms"),
+            "requests": stats["requests"], "rounds": stats["rounds"], "builds_during_stream": stats["builds"] - sum(
+                (cb.need(*w, cb.MODEL_SUBSET) + serve.CHUNK - 1) // serve.CHUNK for w in warm),
+            "resident_gb": stats["resident_gb"], "warmup_and_stream_s": total,
+            "requests_per_s": stats["requests"] / stats["wall_s"],
+            "plain_rebuild_p50_ms": 1e3 * float(np.median(plain)) if plain else None,
+            "plain_sample": len(plain),
+            "note": "n above ~2048 cannot stay resident for d = 2..4 within the budget (a table at n = 16384 is "
+                    "1.07 GB per prime, 14184 primes at d = 3); such requests take the plain path"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -153,6 +191,8 @@ def main():
     ap.add_argument("--d", type=int, default=3)
     ap.add_argument("--batch", type=int, default=0, help="primes per step per GPU (default: one wave)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the served-query latency run")
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the main kernel from an ncu capture (roofline.traffic)")
     a = ap.parse_args()
@@ -270,6 +310,10 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(reference_binary()[0]):
         cpu = cpu_baseline(n, M, d)
+    serving = None
+    if rank == 0 and world == 1 and not a.no_serving:
+        eng.close()  # release the build workspace: the resident tables need the memory
+        serving = serving_run(local, a.serve_seconds)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -282,7 +326,8 @@ def main():
                          "traffic": a.traffic_bytes or MEASURED_TRAFFIC.get((n, M, d, B)),
                          "model": f"{K_OPS_PER_MM} INT32 multiply ops per modular multiplication, "
                                   f"{algorithmic_mm(n):.3e} multiplications per prime-residue; peak measured live"},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary()}))
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+            "serving": serving}))
     if dist:
         dist.destroy_process_group()
     return 0

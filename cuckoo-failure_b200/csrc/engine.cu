@@ -11,6 +11,7 @@
 #include "../../include/cuckoo_b200.h"
 #include "host_common.hpp"
 #include "kernel_lg.cuh"
+#include "table_query.cuh"
 
 using namespace cfb;
 
@@ -152,7 +153,7 @@ static long fit_batch(size_t per_prime) {
 }
 
 static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int d, int model, int J, const Plan& pl,
-                        u64* d_out, cudaStream_t s) {
+                        u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0) {
     const KInfo ki = kernel_for(pl.lg);
     if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ki.smem),
@@ -189,6 +190,8 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
         kp.lay = pl.lay;
         kp.out = d_out + (size_t)at * J;
         kp.err = e->d_err;
+        kp.keep = keep ? keep + (size_t)at * keep_words : nullptr;
+        kp.keep_words = keep_words;
         ki.fn<<<nb, ki.threads, ki.smem, s>>>(kp);
         CF_CUDA(cudaGetLastError(), "kernel launch");
         ++e->launches;
@@ -254,6 +257,122 @@ uint64_t cf_workspace_bytes(int nmax, int Mmax, int J) {
     while ((1ull << lg) < L) ++lg;
     if (lg > MAX_LG) return 0;
     return 8 * make_layout(nmax, F, (int)L, J, warps_for(lg), r_for(lg)).total;
+}
+
+// ---- resident tables (serving) ----
+
+struct cf_tables {
+    int device = 0, n = 0, F = 0, d = 0, d0 = 0, model = 0, B = 0;
+    u64* keep = nullptr;  // [B][keep_words]
+    size_t keep_words = 0;
+    u64* d_primes = nullptr;
+    std::vector<u64> primes;
+    u64* d_out = nullptr;  // [B][jcap] query results
+    int* d_q = nullptr;    // [2][jcap]
+    int jcap = 0;
+};
+
+uint64_t cf_tables_bytes(int nmax, int Fmax) {
+    if (nmax < 1) return 0;
+    return 8 * make_keep_layout(nmax, std::max(nmax, Fmax)).total;
+}
+
+int cf_tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int Fmax, int d, int model, cf_tables** out) {
+    if (!e || !out) return CF_ERR_ARG;
+    *out = nullptr;
+    e->err.clear();
+    e->launches = 0;
+    if (B < 1 || !primes) return fail(e, CF_ERR_ARG, "bad prime buffer");
+    Plan pl;
+    int rc = plan(e, nmax, d, model, nullptr, nullptr, 0, pl);
+    if (rc) return rc;
+    pl.F = std::max(pl.F, Fmax);  // the largest M later queries may use
+    pl.lay = make_layout(nmax, pl.F, 1 << pl.lg, 0, warps_for(pl.lg), r_for(pl.lg));
+    pl.ws_words = pl.lay.total;
+    rc = check_primes(e, primes, B, pl);
+    if (rc) return rc;
+    CF_CUDA(cudaSetDevice(e->device), "set device");
+    cf_tables* t = new cf_tables();
+    t->device = e->device, t->n = nmax, t->F = pl.F, t->d = d, t->d0 = pl.d0, t->model = model, t->B = B;
+    t->keep_words = make_keep_layout(nmax, pl.F).total;
+    t->primes.assign(primes, primes + B);
+    cudaError_t c = cudaMalloc(&t->keep, 8 * t->keep_words * (size_t)B);
+    if (c == cudaSuccess) c = cudaMalloc(&t->d_primes, 8 * (size_t)B);
+    if (c == cudaSuccess) c = cudaMemcpyAsync(t->d_primes, primes, 8 * (size_t)B, cudaMemcpyHostToDevice, e->stream);
+    if (c != cudaSuccess) {
+        cf_tables_free(t);
+        return cuda_fail(e, c, "resident table allocation");
+    }
+    rc = launch_batch(e, t->d_primes, B, nmax, d, model, 0, pl, nullptr, e->stream, t->keep, t->keep_words);
+    if (rc == CF_OK) {
+        int herr = 0;
+        c = cudaMemcpyAsync(&herr, e->d_err, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+        if (c == cudaSuccess) c = cudaStreamSynchronize(e->stream);
+        if (c != cudaSuccess) rc = cuda_fail(e, c, "table build");
+        else if (herr) rc = fail(e, CF_ERR_DEVICE, "device check failed (code " + std::to_string(herr) + ")");
+    }
+    if (rc) {
+        cf_tables_free(t);
+        return rc;
+    }
+    *out = t;
+    return CF_OK;
+}
+
+int cf_tables_query(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, uint64_t* residues) {
+    if (!e || !t) return CF_ERR_ARG;
+    e->err.clear();
+    e->launches = 0;
+    if (J < 1 || !qn || !qM || !residues) return fail(e, CF_ERR_ARG, "bad query buffers");
+    for (int j = 0; j < J; ++j) {
+        if (qn[j] < 1 || qn[j] > t->n || qM[j] <= qn[j] || qM[j] > t->F)
+            return fail(e, CF_ERR_ARG, "query needs 1 <= n <= table n and n < M <= table F");
+        if (t->model == CF_MODEL_SUBSET && t->d > qM[j]) return fail(e, CF_ERR_ARG, "subset model needs d <= M");
+    }
+    CF_CUDA(cudaSetDevice(t->device), "set device");
+    cf_tables* tm = const_cast<cf_tables*>(t);  // the query staging buffers are per table set
+    if (J > tm->jcap) {
+        cudaFree(tm->d_out);
+        cudaFree(tm->d_q);
+        tm->d_out = nullptr;
+        tm->d_q = nullptr;
+        tm->jcap = 0;
+        CF_CUDA(cudaMalloc(&tm->d_out, 8 * (size_t)t->B * J), "query result buffer");
+        CF_CUDA(cudaMalloc(&tm->d_q, sizeof(int) * 2 * (size_t)J), "query buffer");
+        tm->jcap = J;
+    }
+    cudaStream_t s = e->stream;
+    CF_CUDA(cudaMemcpyAsync(tm->d_q, qn, sizeof(int) * J, cudaMemcpyHostToDevice, s), "query upload");
+    CF_CUDA(cudaMemcpyAsync(tm->d_q + J, qM, sizeof(int) * J, cudaMemcpyHostToDevice, s), "query upload");
+    TQParams tp;
+    tp.primes = t->d_primes;
+    tp.B = t->B, tp.n = t->n, tp.F = t->F, tp.d = t->d, tp.d0 = t->d0, tp.model = t->model, tp.J = J;
+    tp.qn = tm->d_q;
+    tp.qM = tm->d_q + J;
+    tp.keep = t->keep;
+    tp.keep_words = t->keep_words;
+    tp.out = tm->d_out;
+    const size_t smem = tq_smem_bytes(t->n);
+    CF_CUDA(cudaFuncSetAttribute((const void*)k_table_query<TQ_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+            "shared memory attribute");
+    k_table_query<TQ_THREADS><<<t->B * J, TQ_THREADS, smem, s>>>(tp);
+    CF_CUDA(cudaGetLastError(), "query launch");
+    ++e->launches;
+    CF_CUDA(cudaMemcpyAsync(residues, tm->d_out, 8 * (size_t)t->B * J, cudaMemcpyDeviceToHost, s), "query download");
+    CF_CUDA(cudaStreamSynchronize(s), "query");
+    return CF_OK;
+}
+
+int cf_tables_count(const cf_tables* t) { return t ? t->B : 0; }
+
+void cf_tables_free(cf_tables* t) {
+    if (!t) return;
+    cudaSetDevice(t->device);
+    cudaFree(t->keep);
+    cudaFree(t->d_primes);
+    cudaFree(t->d_out);
+    cudaFree(t->d_q);
+    delete t;
 }
 
 long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J) {

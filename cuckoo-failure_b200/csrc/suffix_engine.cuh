@@ -224,6 +224,24 @@ CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R) {
 }
 CF_HD int tile_v0(int v) { return 1 + TILE * ((v - 1) / TILE); }  // first column of v's tile
 
+// Resident tables (serving): per prime, the whole V as a packed triangle (row p at p(p-1)/2,
+// entries w = 0..p-1, entries w < d0 unused) and the pair tables fact, ifact, inv up to F, so that
+// later queries (n' <= n, M' <= F) need no rebuild.
+struct KeepLayout {
+    size_t tri, fact, ifact, inv, total;
+};
+CF_HD KeepLayout make_keep_layout(int n, int F) {
+    KeepLayout k;
+    size_t at = 0;
+    k.tri = lay_take(at, (size_t)n * (n + 1) / 2);
+    k.fact = lay_take(at, 2 * ((size_t)F + 1));
+    k.ifact = lay_take(at, 2 * ((size_t)F + 1));
+    k.inv = lay_take(at, 2 * ((size_t)F + 1));
+    k.total = at;
+    return k;
+}
+CF_HD size_t tri_off(size_t p) { return p * (p - 1) / 2; }  // V[p][w] at tri + tri_off(p) + w
+
 // Launch parameters shared by all CTAs of a batch (one CTA per prime).
 struct KParams {
     const u64* primes;  // [B]
@@ -235,6 +253,8 @@ struct KParams {
     Layout lay;         // offsets inside a prime's workspace
     u64* out;           // [B][J] residues
     int* err;           // device error word (0 = ok)
+    u64* keep = nullptr;  // resident tables [B][keep_words] (serving builds), or null
+    size_t keep_words = 0;
 };
 
 // Error codes recorded in *err by the kernel.
@@ -657,6 +677,17 @@ struct PrimeRun {
             }
         });
         fwd_only();
+        if (kp.keep) {  // the pair tables, for queries served later from this prime's resident V
+            const KeepLayout kl = make_keep_layout(n, F);
+            u64* kb = kp.keep + (size_t)b * kp.keep_words;
+            ex.each([&](int t, Regs<G>&) CF_INL {
+                for (size_t k = t; k < 2 * ((size_t)F + 1); k += T) {
+                    kb[kl.fact + k] = fact()[k];
+                    kb[kl.ifact + k] = ifact()[k];
+                    kb[kl.inv + k] = inv()[k];
+                }
+            });
+        }
         ex.each([&](int t, Regs<G>& rg) CF_INL {
             const u64 linv = mi[MI_LINV];
             const u64 linvq = shoup_companion(linv, P);
@@ -840,8 +871,26 @@ struct PrimeRun {
                     }
                 }
             });
+            if (kp.keep) keep_tile(v0, v);
         }
         ex.sync();  // row v + 1 is read by the next step
+    }
+
+    // Serving builds: the tile's columns v0 .. v of V, for every row below them, into the resident
+    // packed triangle.
+    CF_HD void keep_tile(int v0, int v) {
+        const int n = kp.n, d0 = kp.d0, cnt = v - v0 + 1;
+        u64* tri = kp.keep + (size_t)b * kp.keep_words;  // the triangle sits at offset 0
+        ex.each([&](int t, Regs<G>&) CF_INL {
+            for (int r = v0 + 1 + t; r <= n; r += T) {
+                u64* dst = tri + tri_off(r);
+                const u64* src = VS() + r;
+                for (int c = 0; c < cnt; ++c) {
+                    const int w = v0 + c;
+                    if (w >= d0 && w < r) dst[w] = ld_stream(src + (size_t)c * (n + 1));
+                }
+            }
+        });
     }
 
     // Horner finish (fast/cuckoo_fast.cu:877-890):

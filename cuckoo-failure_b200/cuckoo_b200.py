@@ -49,6 +49,15 @@ def lib():
         L.cf_need.restype = ctypes.c_long
         L.cf_lib_primes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u64p, ctypes.c_long]
         L.cf_lib_primes.restype = ctypes.c_long
+        L.cf_tables_bytes.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.cf_tables_bytes.restype = ctypes.c_uint64
+        L.cf_tables_build.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.cf_tables_build.restype = ctypes.c_int
+        L.cf_tables_query.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _intp, _intp, ctypes.c_int, _u64p]
+        L.cf_tables_query.restype = ctypes.c_int
+        L.cf_tables_free.argtypes = [ctypes.c_void_p]
+        L.cf_tables_free.restype = None
         L.cf_transform_length.argtypes = [ctypes.c_uint64]
         L.cf_transform_length.restype = ctypes.c_uint64
         L.cf_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
@@ -156,8 +165,56 @@ class Engine:
                                      ctypes.c_void_p(d_out_ptr), ctypes.c_void_p(stream_ptr or 0))
         self._check(rc)
 
+    def tables(self, primes, nmax, Fmax, d, model=MODEL_SUBSET):
+        """Build and keep the suffix tables of `primes` on the device for later queries."""
+        return Tables(self, primes, nmax, Fmax, d, model)
+
     def max_batch(self, nmax, Mmax, J):
         return int(lib().cf_max_batch(self._h, nmax, Mmax, J))
 
     def last_launches(self):
         return int(lib().cf_last_launches(self._h))
+
+
+class Tables:
+    """Resident tables of a batch of primes (cf_tables_build); query() answers (n, M) with n <= nmax,
+    M <= Fmax from them without a rebuild."""
+
+    def __init__(self, engine, primes, nmax, Fmax, d, model=MODEL_SUBSET):
+        self.engine, self.nmax, self.Fmax, self.d, self.model = engine, nmax, max(nmax, Fmax), d, model
+        self.primes = [int(p) for p in primes]
+        p = np.ascontiguousarray(self.primes, dtype=np.uint64)
+        h = ctypes.c_void_p()
+        rc = lib().cf_tables_build(engine._h, p.ctypes.data_as(_u64p), len(p), nmax, Fmax, d, model, ctypes.byref(h))
+        engine._check(rc)
+        self._t = h
+
+    def query(self, queries):
+        qn, qM = _queries(queries)
+        out = np.zeros((len(self.primes), len(qn)), dtype=np.uint64)
+        rc = lib().cf_tables_query(self.engine._h, self._t, qn.ctypes.data_as(_intp), qM.ctypes.data_as(_intp),
+                                   len(qn), out.ctypes.data_as(_u64p))
+        self.engine._check(rc)
+        return out
+
+    def close(self):
+        if getattr(self, "_t", None):
+            lib().cf_tables_free(self._t)
+            self._t = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def tables_bytes(nmax, Fmax):
+    """Device bytes of one prime's resident table."""
+    return int(lib().cf_tables_bytes(nmax, Fmax))

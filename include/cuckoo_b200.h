@@ -85,6 +85,24 @@ long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J);
 /* Kernel launches issued by the last cf_residues / cf_residues_async call. */
 long cf_last_launches(const cf_engine* e);
 
+/* ---- resident tables for serving (no counterpart in the reference) ----
+ * The reference rebuilds the suffix table for every run.  A served workload keeps, per (d, prime),
+ * the whole table V and the factorial tables on the device, and answers later queries with
+ * n' <= n and M' <= F from them in O(n'^2) per prime, with the same residues
+ * (include/cuckoo/single_table.hpp:103-119 evaluates nbad from a retained table the same way). */
+typedef struct cf_tables cf_tables;
+
+/* Device bytes one prime's resident table takes for tables up to nmax and M up to Fmax. */
+uint64_t cf_tables_bytes(int nmax, int Fmax);
+/* Build and keep the tables of B primes (same requirements as cf_residues, with every prime above
+ * Fmax).  Returns when they are on the device; *out owns that memory until cf_tables_free. */
+int cf_tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int Fmax, int d, int model, cf_tables** out);
+/* residues[b*J + j] = N_bad(qn[j], qM[j]) mod primes[b] for the table set's primes, 1 <= qn[j] <= nmax,
+ * qn[j] < qM[j] <= Fmax.  Host buffers; returns when the residues are in `residues`. */
+int cf_tables_query(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, uint64_t* residues);
+int cf_tables_count(const cf_tables* t);
+void cf_tables_free(cf_tables* t);
+
 /* ---- allocation-free variant (no counterpart in the reference) ---- */
 
 /* Bytes of the static device scratch used by cf_residues_noalloc (64 MiB).  One prime's table

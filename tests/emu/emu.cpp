@@ -84,9 +84,27 @@ extern "C" long emu_block_cell(int P, int W, int h) { return (long)block_cell(P,
 extern "C" long emu_block_count(int n) { return (long)block_count(n); }
 extern "C" int emu_block_h(int n) { return block_h(n); }
 
+static int emu_run(const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM, int J,
+                   uint64_t* out, int Fmin, std::vector<u64>* keep);
+
 extern "C" int emu_residues(const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM, int J,
                             uint64_t* out) {
-    int F = nmax;
+    return emu_run(primes, B, nmax, d, model, qn, qM, J, out, 0, nullptr);
+}
+
+// A serving build of one prime (no queries): copies out the resident table (the packed triangle
+// of folded V, then fact, ifact, inv pairs up to F) into keep_out[keep_words].
+extern "C" long emu_keep_words(int nmax, int F) { return (long)make_keep_layout(nmax, F).total; }
+extern "C" int emu_keep_build(uint64_t prime, int nmax, int Fmin, int d, int model, uint64_t* keep_out) {
+    std::vector<u64> keep;
+    const int rc = emu_run(&prime, 1, nmax, d, model, nullptr, nullptr, 0, nullptr, Fmin, &keep);
+    if (rc == 0) std::memcpy(keep_out, keep.data(), keep.size() * sizeof(u64));
+    return rc;
+}
+
+static int emu_run(const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM, int J,
+                   uint64_t* out, int Fmin, std::vector<u64>* keep) {
+    int F = nmax > Fmin ? nmax : Fmin;
     for (int j = 0; j < J; ++j) F = qM[j] > F ? qM[j] : F;
     if (model == MODEL_SUBSET && d > F) F = d;
     const int L = (int)cfh::transform_length((uint64_t)nmax);
@@ -113,6 +131,11 @@ extern "C" int emu_residues(const uint64_t* primes, int B, int nmax, int d, int 
     kp.lay = lo;
     kp.out = out;
     kp.err = &err;
+    if (keep) {  // poisoned too: entries the build never writes must never be read by a query
+        keep->assign(make_keep_layout(nmax, F).total * (size_t)B, 0xA5A5A5A5A5A5A5A5ull);
+        kp.keep = keep->data();
+        kp.keep_words = make_keep_layout(nmax, F).total;
+    }
     switch (lg) {
         case 4: run_lg<4>(kp); break;
         case 5: run_lg<5>(kp); break;

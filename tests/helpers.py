@@ -79,6 +79,10 @@ def emu():
         L.emu_residues.argtypes = [ctypes.POINTER(u64), ci, ci, ci, ci, ctypes.POINTER(ci), ctypes.POINTER(ci), ci,
                                    ctypes.POINTER(u64)]
         L.emu_residues.restype = ci
+        L.emu_keep_words.argtypes = [ci, ci]
+        L.emu_keep_words.restype = ctypes.c_long
+        L.emu_keep_build.argtypes = [u64, ci, ci, ci, ci, ctypes.POINTER(u64)]
+        L.emu_keep_build.restype = ci
         L.emu_block_cell.argtypes = [ci, ci, ci]
         L.emu_block_cell.restype = ctypes.c_long
         L.emu_block_count.argtypes = [ci]
