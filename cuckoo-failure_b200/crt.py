@@ -70,6 +70,69 @@ def crt(pairs):
     return items[0]
 
 
+class PrefixCRT:
+    """CRT over prefixes of one fixed prime list, with the big-integer constants cached.
+
+    Every query's primes are primes number 0 .. k-1 of the same list, so the merge tree can be
+    fixed once: [0, k) splits into dyadic blocks [s, s + 2^l) (the binary digits of k, largest
+    first), each block merges its halves recursively, and the blocks merge left to right.  The
+    block products and the modular inverses of each merge (m_left^-1 mod m_right) depend only on
+    the list, so they are computed once and reused; a query then costs multiplications and
+    reductions only, no extended Euclid.  The result equals crt() (both are the canonical residue)."""
+
+    def __init__(self, primes):
+        self.p = [int(q) for q in primes]
+        self._prod = {}
+        self._inv = {}
+
+    def prod(self, lo, hi):
+        key = (lo, hi)
+        m = self._prod.get(key)
+        if m is None:
+            if hi - lo == 1:
+                m = self.p[lo]
+            else:
+                mid = (lo + hi) // 2
+                m = self.prod(lo, mid) * self.prod(mid, hi)
+            self._prod[key] = m
+        return m
+
+    def _merge_inv(self, key, ml, mr):
+        v = self._inv.get(key)
+        if v is None:
+            v = pow(ml % mr, -1, mr)
+            self._inv[key] = v
+        return v
+
+    def _block(self, lo, hi, r):
+        if hi - lo == 1:
+            return r[lo] % self.p[lo]
+        mid = (lo + hi) // 2
+        xl, xr = self._block(lo, mid, r), self._block(mid, hi, r)
+        ml, mr = self.prod(lo, mid), self.prod(mid, hi)
+        return xl + ml * ((xr - xl) * self._merge_inv(("b", lo, hi), ml, mr) % mr)
+
+    def crt(self, residues):
+        """(x, m) for residues r_0 .. r_{k-1} modulo primes 0 .. k-1 of the list."""
+        r = [int(v) for v in residues]
+        k = len(r)
+        if k > len(self.p):
+            raise ValueError("more residues than primes")
+        x, m, s = 0, 1, 0
+        for lvl in range(k.bit_length() - 1, -1, -1):
+            if not (k >> lvl) & 1:
+                continue
+            e = s + (1 << lvl)
+            xb, mb = self._block(s, e, r), self.prod(s, e)
+            if s == 0:
+                x, m = xb, mb
+            else:
+                x = x + m * ((xb - x) * self._merge_inv(("p", s, e), m, mb) % mb)
+                m = m * mb
+            s = e
+        return x, m
+
+
 def q_power(n, M, d, replacement=False):
     """Q^n exactly: C(M, d)^n, or (M^d)^n for the replacement model."""
     return (M**d if replacement else math.comb(M, d)) ** n

@@ -12,9 +12,13 @@ recently used.
 
 Each round of the loop takes every request that has arrived (continuous batching: requests
 arriving while the GPU works join the next round), builds the chunks the round is missing, and
-answers all of the round's requests per chunk with one query launch.  Latency is measured from
-a request's arrival to the end of its CRT.  A request whose tables cannot be resident within
-the budget is computed the plain way (cf_residues, no residency) in its round.
+answers all of the round's requests per chunk with one query launch.  A request whose tables
+cannot be resident within the budget is computed the plain way (cf_residues, no residency) in
+its round.  The residues of a served request cover whole chunks (the primes beyond its need
+change nothing: N_bad is below the product of its own primes), so every CRT is over a prefix of
+the list whose length is a multiple of the chunk, and a pool of host processes (crt.PrefixCRT,
+constants cached at start) recombines them while the GPU serves the next round.  Two latencies
+are kept per request, from its arrival: residues ready, and N_bad ready.
 
     python cuckoo-failure_b200/serve.py [--seconds 10] [--rate 200] [--nmax 2048] [--budget-gb 150] [--seed 1]
 """
@@ -107,7 +111,8 @@ class Server:
         return True
 
     def round(self, reqs):
-        """Answer a batch of requests [(id, n, M, d)] -> {id: N_bad}."""
+        """Residues for a batch of requests [(id, n, M, d)] -> {id: [residue modulo prime i, i = 0, 1, ...]}
+        covering at least the request's need(n, M, d) primes (whole chunks when served resident)."""
         res = {rid: {} for rid, _, _, _ in reqs}
         plain = []
         # which chunks each request needs
@@ -130,30 +135,73 @@ class Server:
             tab = self.chunks[(d, c)]
             out = tab.query([(n, M) for _, n, M in items])
             for jj, (rid, n, M) in enumerate(items):
-                k = need[rid]
-                for b, p in enumerate(tab.primes):
-                    if c * self.chunk + b < k:
-                        res[rid][p] = int(out[b, jj])
+                col = out[:, jj]
+                for b in range(len(tab.primes)):
+                    res[rid][c * self.chunk + b] = int(col[b])
         for rid, n, M, d in reqs:
             if rid in bad:
                 plain.append((rid, n, M, d))
         for rid, n, M, d in plain:  # no residency: rebuild for this request alone
             ps = cb.prime_range(0, need[rid])
             r = self.eng.residues(ps, n, d, [(n, M)], model=self.model)
-            res[rid] = {int(p): int(x) for p, x in zip(ps, r[:, 0])}
+            res[rid] = {i: int(x) for i, x in enumerate(r[:, 0])}
             self.plain += 1
-        return {rid: crt.crt(list(v.items()))[0] for rid, v in res.items()}
+        return {rid: [v[i] for i in range(len(v))] for rid, v in res.items()}
 
 
-def run(stream, engine, budget_bytes, model=cb.MODEL_SUBSET, warm=None, max_round=512, chunk=CHUNK):
+# ---- host CRT workers (separate processes, started with spawn) ----
+_PCRT = None
+
+
+def _crt_init(primes, warm_lengths):
+    global _PCRT
+    _PCRT = crt.PrefixCRT(primes)
+    for k in warm_lengths:
+        _PCRT.crt([0] * k)
+
+
+def _crt_job(residues):
+    return _PCRT.crt(residues)[0]
+
+
+def crt_pool(max_primes, chunk=CHUNK, workers=None):
+    """Process pool whose workers hold crt.PrefixCRT over the fixed list, its constants for every
+    chunk-multiple prefix computed before the pool is returned."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    workers = workers or max(1, min(16, (os.cpu_count() or 2) - 1))
+    kmax = ((max_primes + chunk - 1) // chunk) * chunk
+    primes = [int(p) for p in cb.prime_range(0, kmax)]
+    warm = list(range(chunk, kmax + 1, chunk))
+    pool = cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"),
+                                  initializer=_crt_init, initargs=(primes, warm))
+    list(pool.map(time.sleep, [0.05] * (2 * workers)))  # every worker started and warm
+    return pool
+
+
+def run(stream, engine, budget_bytes, model=cb.MODEL_SUBSET, warm=None, max_round=512, chunk=CHUNK, pool=None):
     """Serve a timed stream [(arrival_s, n, M, d)] in real time.  `warm`, if given, is a list of
-    (n, M, d) built before the clock starts.  Returns (latencies_s, results, stats)."""
+    (n, M, d) built before the clock starts.  Returns (latencies_s, results, stats): the latency to
+    N_bad per request, N_bad per request, and counters including the latency to residues."""
     srv = Server(engine, budget_bytes, model, chunk=chunk)
     for n, M, d in warm or []:
         for c in range((cb.need(n, M, d, model) + chunk - 1) // chunk):
             srv._ensure(d, c, n, M, set())
+    own_pool = pool is None
+    if own_pool:
+        kmax = max([cb.need(n, M, d, model) for _, n, M, d in stream] + [1])
+        pool = crt_pool(kmax, chunk)
+    futs = [None] * len(stream)
+    lat, res_lat = [0.0] * len(stream), [0.0] * len(stream)
     t0 = time.perf_counter()
-    lat, results, rounds, i = [0.0] * len(stream), [None] * len(stream), 0, 0
+    gpu_s, rounds, i = 0.0, 0, 0
+
+    def stamp(k):
+        def cb_(_f):
+            lat[k] = time.perf_counter() - t0 - stream[k][0]
+        return cb_
+
     while i < len(stream):
         now = time.perf_counter() - t0
         if stream[i][0] > now:
@@ -163,18 +211,25 @@ def run(stream, engine, budget_bytes, model=cb.MODEL_SUBSET, warm=None, max_roun
         while j < len(stream) and stream[j][0] <= now and j - i < max_round:
             j += 1
         batch = [(k, stream[k][1], stream[k][2], stream[k][3]) for k in range(i, j)]
+        g0 = time.perf_counter()
         out = srv.round(batch)
         done = time.perf_counter() - t0
+        gpu_s += time.perf_counter() - g0
         for k, _, _, _ in batch:
-            lat[k] = done - stream[k][0]
-            results[k] = out[k]
+            res_lat[k] = done - stream[k][0]
+            futs[k] = pool.submit(_crt_job, out[k])
+            futs[k].add_done_callback(stamp(k))
         rounds += 1
         i = j
+    results = [f.result() for f in futs]
     wall = time.perf_counter() - t0
     stats = {"requests": len(stream), "rounds": rounds, "builds": srv.builds, "plain": srv.plain,
-             "resident_gb": srv.used / 1e9, "wall_s": wall}
+             "resident_gb": srv.used / 1e9, "wall_s": wall, "engine_s": gpu_s,
+             "residues_latency": percentiles(res_lat)}
     for tab in srv.chunks.values():
         tab.close()
+    if own_pool:
+        pool.shutdown()
     return lat, results, stats
 
 

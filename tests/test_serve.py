@@ -63,15 +63,29 @@ def test_rounds_match_requests_alone_with_eviction_and_plain_path():
     for k in range(18):
         n = int(rng.integers(8, 48))
         reqs.append((k, n, int(n * rng.uniform(1.5, 3.5)) + 1, int(rng.choice([2, 3]))))
+    pc = crt.PrefixCRT(cb.prime_range(0, 64))
     got = {}
     for i in range(0, len(reqs), 6):  # three rounds
         got.update(srv.round(reqs[i:i + 6]))
     for rid, n, M, d in reqs:
-        assert got[rid] == alone(n, M, d), (rid, n, M, d)
+        assert len(got[rid]) >= cb.need(n, M, d)
+        assert pc.crt(got[rid])[0] == alone(n, M, d), (rid, n, M, d)
     assert srv.builds > 0 and srv.used <= budget
     # a request far too large for the budget goes the plain way and is still exact
     big = serve.Server(eng, 1, chunk=4)
-    assert big.round([(0, 30, 70, 3)])[0] == alone(30, 70, 3) and big.plain == 1
+    r = big.round([(0, 30, 70, 3)])[0]
+    assert pc.crt(r)[0] == alone(30, 70, 3) and big.plain == 1
+
+
+def test_prefix_crt_equals_pairwise_crt():
+    import random
+
+    ps = cb.prime_range(0, 300)
+    pc = crt.PrefixCRT(ps)
+    rng = random.Random(3)
+    for k in (1, 2, 3, 7, 64, 100, 255, 256, 257, 300):
+        rs = [rng.randrange(p) for p in ps[:k]]
+        assert pc.crt(rs) == crt.crt(list(zip(ps[:k], rs)))
 
 
 @pytest.mark.gpu
@@ -84,3 +98,14 @@ def test_served_results_equal_alone_on_gpu():
             r = eng.residues(ps, n, d, [(n, M)])
             assert x == crt.crt(list(zip(ps, (int(v) for v in r[:, 0]))))[0], (n, M, d)
     assert stats["requests"] == len(stream) and all(v > 0 for v in lat)
+
+
+def test_run_loop_with_crt_pool():
+    """The timed loop end to end (continuous batching, spawn pool for CRT) with the oracle engine."""
+    stream = [(0.01 * k, n, M, d) for k, (n, M, d) in enumerate([(12, 30, 2), (20, 41, 3), (9, 20, 3), (30, 60, 2),
+                                                                  (16, 40, 3), (25, 70, 2)])]
+    lat, res, stats = serve.run(stream, OracleEngine(), 10**9, chunk=8)
+    for (t, n, M, d), x in zip(stream, res):
+        assert x == alone(n, M, d)
+    assert stats["requests"] == 6 and all(v > 0 for v in lat)
+    assert stats["residues_latency"]["p50_ms"] > 0
