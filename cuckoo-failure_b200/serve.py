@@ -135,18 +135,16 @@ class Server:
             tab = self.chunks[(d, c)]
             out = tab.query([(n, M) for _, n, M in items])
             for jj, (rid, n, M) in enumerate(items):
-                col = out[:, jj]
-                for b in range(len(tab.primes)):
-                    res[rid][c * self.chunk + b] = int(col[b])
+                res[rid][c] = out[:, jj].tolist()  # primes c*chunk .. c*chunk + chunk - 1
         for rid, n, M, d in reqs:
             if rid in bad:
                 plain.append((rid, n, M, d))
         for rid, n, M, d in plain:  # no residency: rebuild for this request alone
             ps = cb.prime_range(0, need[rid])
             r = self.eng.residues(ps, n, d, [(n, M)], model=self.model)
-            res[rid] = {i: int(x) for i, x in enumerate(r[:, 0])}
+            res[rid] = {0: r[:, 0].tolist()}
             self.plain += 1
-        return {rid: [v[i] for i in range(len(v))] for rid, v in res.items()}
+        return {rid: [x for c in sorted(v) for x in v[c]] for rid, v in res.items()}
 
 
 # ---- host CRT workers (separate processes, started with spawn) ----
