@@ -2,13 +2,15 @@
 // with the GPU behind the C ABI of include/cuckoo_b200.h.  Same command line, same resume rules,
 // same output lines, so fast/post_gmp.py (or this package's crt.py, which needs no gmpy2) combines the residues as before.
 //
-//   cuckoo_fast_b200 D QUERIES FIRST COUNT [--batch B] [--out FILE] [--device N] [--replacement]
+//   cuckoo_fast_b200 D QUERIES FIRST COUNT [--batch B] [--out FILE] [--device N] [--replacement] [--prime-bits 62]
 //
 // QUERIES: lines "n M".  Prime number i is the i-th largest prime p < 2^50 with 2^20 | p - 1.  A
 // query is evaluated for prime i only if i < need(n, M).  Output lines: "i p n M residue".  With
 // --out the file is appended to and primes already complete in it are skipped.
 // --replacement selects the model with d independent draws (Q = M^d, the library's
 // OneTableModel::replacement); the reference's fast engine has only the d-subset model.
+// --prime-bits 62 uses the prime list below 2^62 and need() over 61 bits, the output of the
+// reference built with -DFP_RB=64 (fast/cuckoo_fast.cu:48-57); combine with --pbits 61.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -27,19 +29,23 @@ struct Query {
 
 int main(int argc, char** argv) {
     if (argc < 5) {
-        std::fprintf(stderr, "usage: cuckoo_fast_b200 D QUERIES FIRST COUNT [--batch B] [--out FILE] [--device N] [--replacement]\n");
+        std::fprintf(stderr, "usage: cuckoo_fast_b200 D QUERIES FIRST COUNT [--batch B] [--out FILE] [--device N] [--replacement] [--prime-bits 62]\n");
         return 2;
     }
     const int d = std::atoi(argv[1]);
     const long first = std::atol(argv[3]), count = std::atol(argv[4]);
     long batch = 0;
-    int device = 0, model = CF_MODEL_SUBSET;
+    int device = 0, model = CF_MODEL_SUBSET, bits = cfh::PRIME_BITS;
     const char* out_path = nullptr;
     for (int i = 5; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--batch") && i + 1 < argc) batch = std::atol(argv[++i]);
         else if (!std::strcmp(argv[i], "--out") && i + 1 < argc) out_path = argv[++i];
         else if (!std::strcmp(argv[i], "--device") && i + 1 < argc) device = std::atoi(argv[++i]);
         else if (!std::strcmp(argv[i], "--replacement")) model = CF_MODEL_REPLACEMENT;
+        else if (!std::strcmp(argv[i], "--prime-bits") && i + 1 < argc && (bits = std::atoi(argv[++i])) != 50 && bits != 62) {
+            std::fprintf(stderr, "--prime-bits takes 50 or 62\n");
+            return 2;
+        }
         else {
             std::fprintf(stderr, "unknown option %s\n", argv[i]);
             return 2;
@@ -61,7 +67,7 @@ int main(int argc, char** argv) {
                 std::fclose(f);
                 return 2;
             }
-            qs.push_back({n, M, cf_need(n, M, d, model)});
+            qs.push_back({n, M, cf_need_bits(n, M, d, model, bits)});
             nmax = std::max(nmax, n);
             Mmax = std::max(Mmax, M);
             maxneed = std::max(maxneed, qs.back().need);
@@ -108,9 +114,9 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "nothing to do (%zu primes already in the output)\n", done.size());
         return 0;
     }
-    const std::vector<uint64_t> primes = cfh::prime_range(first, count);  // primes[i - first]
-    if (primes.empty() || primes.back() < (1ull << (cfh::PRIME_BITS - 1))) {
-        std::fprintf(stderr, "prime list exhausted above 2^%d\n", cfh::PRIME_BITS - 1);
+    const std::vector<uint64_t> primes = cfh::prime_range(first, count, bits);  // primes[i - first]
+    if (primes.empty() || primes.back() < (1ull << (bits - 1))) {
+        std::fprintf(stderr, "prime list exhausted above 2^%d\n", bits - 1);
         return 4;
     }
 
@@ -128,7 +134,7 @@ int main(int argc, char** argv) {
     }
     const size_t B = (size_t)std::min<long>(batch, (long)todo.size());
     std::fprintf(stderr, "[cuda-b200] %d-bit primes, d=%d, %s, nmax=%d, L=%llu, %.3f GB per prime, batch %zu, %zu primes to do\n",
-                 cfh::PRIME_BITS, d, model == CF_MODEL_SUBSET ? "d-subset" : "replacement", nmax,
+                 bits, d, model == CF_MODEL_SUBSET ? "d-subset" : "replacement", nmax,
                  (unsigned long long)cf_transform_length((uint64_t)nmax), per_prime / 1073741824.0, B, todo.size());
 
     const auto t0 = std::chrono::steady_clock::now();

@@ -26,7 +26,33 @@ cfb::KInfo cf_kinfo_lg11();
 cfb::KInfo cf_kinfo_lg12();
 cfb::KInfo cf_kinfo_lg13();
 cfb::KInfo cf_kinfo_lg14();
-static KInfo kernel_for(int lg) {
+cfb::KInfo cf_kinfo_lg4_w();
+cfb::KInfo cf_kinfo_lg5_w();
+cfb::KInfo cf_kinfo_lg6_w();
+cfb::KInfo cf_kinfo_lg7_w();
+cfb::KInfo cf_kinfo_lg8_w();
+cfb::KInfo cf_kinfo_lg9_w();
+cfb::KInfo cf_kinfo_lg10_w();
+cfb::KInfo cf_kinfo_lg11_w();
+cfb::KInfo cf_kinfo_lg12_w();
+cfb::KInfo cf_kinfo_lg13_w();
+cfb::KInfo cf_kinfo_lg14_w();
+// The kernel for transform length 2^lg: primes below 2^50, or (wide) below 2^62.
+static KInfo kernel_for(int lg, bool wide = false) {
+    if (wide) switch (lg) {
+            case 4: return cf_kinfo_lg4_w();
+            case 5: return cf_kinfo_lg5_w();
+            case 6: return cf_kinfo_lg6_w();
+            case 7: return cf_kinfo_lg7_w();
+            case 8: return cf_kinfo_lg8_w();
+            case 9: return cf_kinfo_lg9_w();
+            case 10: return cf_kinfo_lg10_w();
+            case 11: return cf_kinfo_lg11_w();
+            case 12: return cf_kinfo_lg12_w();
+            case 13: return cf_kinfo_lg13_w();
+            case 14: return cf_kinfo_lg14_w();
+            default: return KInfo{nullptr, 0, 0, 0};
+        }
     switch (lg) {
         case 4: return cf_kinfo_lg4();
         case 5: return cf_kinfo_lg5();
@@ -60,6 +86,7 @@ struct cf_engine {
     size_t io_cap = 0;  // primes capacity of d_primes; d_out has io_cap * jcap
     int jcap = 0;
     long launches = 0;
+    int prime_bits = 50;  // for cf_residues_async, whose primes are not read on the host
     std::string err;
 };
 
@@ -78,6 +105,7 @@ static int cuda_fail(cf_engine* e, cudaError_t c, const char* what) {
 
 struct Plan {
     int lg, F, d0;
+    bool wide = false;  // some prime is 2^50 or above: the kernels for primes below 2^62
     Layout lay;
     size_t ws_words;
 };
@@ -111,12 +139,14 @@ static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const i
     return CF_OK;
 }
 
-static int check_primes(cf_engine* e, const u64* primes, int B, const Plan& pl) {
+static int check_primes(cf_engine* e, const u64* primes, int B, Plan& pl) {
     const u64 L = 1ull << pl.lg;
+    pl.wide = false;
     for (int b = 0; b < B; ++b) {
         const u64 p = primes[b];
-        if (p < 3 || (p & 1) == 0 || p >= (1ull << 50) || p <= (u64)pl.F || (p - 1) % L != 0 || !cfh::is_prime(p))
-            return fail(e, CF_ERR_ARG, "prime " + std::to_string(p) + " is not an odd prime < 2^50 above max(n, M) with L | p-1");
+        if (p < 3 || (p & 1) == 0 || p >= (1ull << 62) || p <= (u64)pl.F || (p - 1) % L != 0 || !cfh::is_prime(p))
+            return fail(e, CF_ERR_ARG, "prime " + std::to_string(p) + " is not an odd prime < 2^62 above max(n, M) with L | p-1");
+        if (p >= (1ull << 50)) pl.wide = true;
     }
     return CF_OK;
 }
@@ -154,7 +184,7 @@ static long fit_batch(size_t per_prime) {
 
 static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int d, int model, int J, const Plan& pl,
                         u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0) {
-    const KInfo ki = kernel_for(pl.lg);
+    const KInfo ki = kernel_for(pl.lg, pl.wide);
     if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ki.smem),
             "shared memory attribute");
@@ -208,6 +238,21 @@ long cf_prime_range(long first, long count, uint64_t* out) {
     return (long)v.size();
 }
 long cf_need(int n, int M, int d, int model) { return cfh::need(n, M, d, model); }
+long cf_prime_range_bits(long first, long count, int bits, uint64_t* out) {
+    if ((bits != 50 && bits != 62) || first < 0 || count < 0 || (count > 0 && !out)) return 0;
+    const std::vector<u64> v = cfh::prime_range(first, count, bits);
+    std::copy(v.begin(), v.end(), out);
+    return (long)v.size();
+}
+long cf_need_bits(int n, int M, int d, int model, int bits) {
+    if (bits != 50 && bits != 62) return -1;
+    return cfh::need(n, M, d, model, bits);
+}
+int cf_engine_set_prime_bits(cf_engine* e, int bits) {
+    if (!e || (bits != 50 && bits != 62)) return CF_ERR_ARG;
+    e->prime_bits = bits;
+    return CF_OK;
+}
 long cf_lib_primes(int n, int M, int d, int model, uint64_t* out, long cap) {
     if (n < 1 || M < 1 || d < 1 || (model == CF_MODEL_SUBSET && d > M) || cap < 0 || (cap > 0 && !out)) return -1;
     const std::vector<u64> v = cfh::lib_primes_for(n, M, d, model);
@@ -291,6 +336,7 @@ int cf_tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int F
     pl.ws_words = pl.lay.total;
     rc = check_primes(e, primes, B, pl);
     if (rc) return rc;
+    if (pl.wide) return fail(e, CF_ERR_UNSUPPORTED, "resident tables hold primes below 2^50");
     CF_CUDA(cudaSetDevice(e->device), "set device");
     cf_tables* t = new cf_tables();
     t->device = e->device, t->n = nmax, t->F = pl.F, t->d = d, t->d0 = pl.d0, t->model = model, t->B = B;
@@ -393,6 +439,7 @@ int cf_residues_async(cf_engine* e, const uint64_t* d_primes, int B, int nmax, i
     int rc = plan(e, nmax, d, model, qn, qM, J, pl);
     if (rc) return rc;
     if (B == 0) return CF_OK;
+    pl.wide = e->prime_bits > 50;
     CF_CUDA(cudaSetDevice(e->device), "set device");
     cudaStream_t s = (cudaStream_t)stream;  // NULL is the CUDA default stream
     rc = ensure_queries(e, qn, qM, J, s);

@@ -46,12 +46,14 @@ inline bool is_prime(u64 n) {
 
 constexpr int PRIME_BITS = 50;  // primes of the fixed list lie in (2^49, 2^50)
 constexpr int TWO_ADIC = 20;    // and have 2^20 | p - 1
+// The reference's -DFP_RB=64 build uses the list below 2^62 instead (fast/cuckoo_fast.cu:48-57):
+// `bits` = 50 or 62 in the two functions below.
 
 // Primes number first .. first+count-1 of the fixed list, largest first (fast/cuckoo_fast.cu:422-432).
-inline std::vector<u64> prime_range(long first, long count) {
+inline std::vector<u64> prime_range(long first, long count, int bits = PRIME_BITS) {
     std::vector<u64> out;
     long idx = 0;
-    for (u64 c = ((1ull << PRIME_BITS) - 2) >> TWO_ADIC; c >= 1 && (long)out.size() < count; --c) {
+    for (u64 c = ((1ull << bits) - 2) >> TWO_ADIC; c >= 1 && (long)out.size() < count; --c) {
         const u64 p = (c << TWO_ADIC) + 1;
         if (!is_prime(p)) continue;
         if (idx++ >= first) out.push_back(p);
@@ -67,9 +69,10 @@ inline double log2_Q(int M, int d, int model) {
     for (int i = 0; i < d; ++i) b += std::log2((long double)(M - i)) - std::log2((long double)(i + 1));
     return (double)b;
 }
-// Primes a query needs: the product of that many primes (each > 2^49) exceeds 4 Q^n (fast/cuckoo_fast.cu:457-459).
-inline long need(int n, int M, int d, int model) {
-    return (long)std::ceil(((long double)n * log2_Q(M, d, model) + 3) / (PRIME_BITS - 1)) + 1;
+// Primes a query needs: the product of that many primes (each > 2^(bits-1)) exceeds 4 Q^n
+// (fast/cuckoo_fast.cu:457-459).
+inline long need(int n, int M, int d, int model, int bits = PRIME_BITS) {
+    return (long)std::ceil(((long double)n * log2_Q(M, d, model) + 3) / (bits - 1)) + 1;
 }
 inline u64 transform_length(u64 nmax) {
     u64 L = 1;

@@ -2,3 +2,4 @@
 #include "kernel_lg.cuh"
 
 cfb::KInfo cf_kinfo_lg9() { return cfb::kinfo<9>(); }
+cfb::KInfo cf_kinfo_lg9_w() { return cfb::kinfo<9, true>(); }

@@ -2,3 +2,4 @@
 #include "kernel_lg.cuh"
 
 cfb::KInfo cf_kinfo_lg11() { return cfb::kinfo<11>(); }
+cfb::KInfo cf_kinfo_lg11_w() { return cfb::kinfo<11, true>(); }

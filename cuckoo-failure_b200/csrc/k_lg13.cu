@@ -2,3 +2,4 @@
 #include "kernel_lg.cuh"
 
 cfb::KInfo cf_kinfo_lg13() { return cfb::kinfo<13>(); }
+cfb::KInfo cf_kinfo_lg13_w() { return cfb::kinfo<13, true>(); }

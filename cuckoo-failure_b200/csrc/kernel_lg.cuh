@@ -88,12 +88,12 @@ struct DevExec {
     }
 };
 
-template <int LG, int R>
+template <int LG, int R, bool W>
 __global__ void __launch_bounds__(Geo<LG, R>::T) k_suffix(KParams kp) {
     typedef Geo<LG, R> G;
     extern __shared__ __align__(16) u64 smem[];
     DevExec<G> ex;
-    PrimeRun<G, DevExec<G>> pr(ex, kp, (int)blockIdx.x, smem);
+    PrimeRun<G, DevExec<G>, W> pr(ex, kp, (int)blockIdx.x, smem);
     pr.run();
 }
 
@@ -111,10 +111,11 @@ struct KInfo {
     size_t smem;
     int r;  // log2 of the entries per thread
 };
-template <int LG>
+// W selects the kernel for primes below 2^62 (otherwise below 2^50).
+template <int LG, bool W = false>
 inline KInfo kinfo() {
     typedef Geo<LG, RFor<LG>::R> G;
-    return KInfo{&k_suffix<LG, RFor<LG>::R>, G::T, Smem<G>::BYTES, RFor<LG>::R};
+    return KInfo{&k_suffix<LG, RFor<LG>::R, W>, G::T, Smem<G>::BYTES, RFor<LG>::R};
 }
 
 }  // namespace cfb

@@ -278,7 +278,12 @@ struct Regs {
     u64 x[G::E];
 };
 
-template <class G, class X>
+// W = false: primes below 2^50 (the fixed list of fast/cuckoo_fast.cu with FP_RB = 52); transform
+// values stay lazily reduced in [0, 4p) forward and [0, 8p) inverse.
+// W = true: primes below 2^62 (the list of the FP_RB = 64 build); with 8p beyond 2^64 every
+// transform value stays in [0, 2p) instead (one more conditional subtraction per output), and the
+// few products whose lazy factor could reach 2^62 take a canonical one.
+template <class G, class X, bool W = false>
 struct PrimeRun {
     static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP, NW = G::NW;
     // L = 2^14 (512 threads x 32 entries): the kernel spectrum lives in tensor memory, each thread's
@@ -383,7 +388,7 @@ struct PrimeRun {
         typedef Plan<PASS, FWD> PL;
         constexpr int D = PIPE_D;
         const int off = PL::bb ? (t & ((1 << PL::bb) - 1)) : 0;
-        const u64 P4 = 4 * P;
+        const u64 P4 = 4 * P, P2 = 2 * P;
         u64 rw[D + 1], rq[D + 1];
         window<D, 0>([&](auto fc) CF_INL {
             constexpr int f = decltype(fc)::value;
@@ -399,7 +404,23 @@ struct PrimeRun {
                 pin(x[j0]);
                 pin(x[j1]);
                 const u64 w = rw[f % (D + 1)], wq = rq[f % (D + 1)];
-                if constexpr (FWD) {
+                if constexpr (FWD && W) {  // inputs and outputs in [0, 2p)
+                    const u64 a = x[j0], c = x[j1];
+                    x[j0] = red2(a + c, P2);
+                    const u64 dd = a - c + P2;
+                    x[j1] = red2(trivial ? dd : shoup_mul_lazy(dd, w, wq, P), P2);
+                } else if constexpr (W) {
+                    const u64 a = x[j0];
+                    if constexpr (trivial) {
+                        const u64 c = x[j1];
+                        x[j0] = red2(a + c, P2);
+                        x[j1] = red2(a - c + P2, P2);
+                    } else {
+                        const u64 c = red2(shoup_mul_lazy(x[j1], w, wq, P), P2);  // -w_{2h}^{-j} y
+                        x[j0] = red2(a - c + P2, P2);
+                        x[j1] = red2(a + c, P2);
+                    }
+                } else if constexpr (FWD) {
                     const u64 a = x[j0], c = x[j1];
                     x[j0] = red2(a + c, P4);
                     const u64 dd = a - c + P4;
@@ -474,6 +495,7 @@ struct PrimeRun {
             for (int k = 0; k < 4; ++k) {
                 const u64 w = (u64)cur[4 * k] | ((u64)cur[4 * k + 1] << 32), wq = (u64)cur[4 * k + 2] | ((u64)cur[4 * k + 3] << 32);
                 x[4 * C + k] = shoup_mul_lazy(x[4 * C + k], w, wq, P);
+                if constexpr (W) x[4 * C + k] = red2(x[4 * C + k], 2 * P);
             }
             ex.tmem_wait_ld();
             tm_pointwise<C + 1>(t, ta, x, b0, b1);
@@ -495,6 +517,7 @@ struct PrimeRun {
                 constexpr int j = decltype(jc)::value;
                 pin(x[j]);
                 x[j] = shoup_mul_lazy(x[j], w, wq, P);
+                if constexpr (W) x[j] = red2(x[j], 2 * P);
             },
             [&](auto jc) CF_INL { pin(x[decltype(jc)::value]); });
     }
@@ -745,7 +768,10 @@ struct PrimeRun {
                     },
                     [&](auto jc, u64 c, u64 cq) CF_INL {
                         constexpr int j = decltype(jc)::value;
-                        if (G::idx(0, t, j) < q) acc += shoup_mul_lazy(rg.x[j], c, cq, P);  // < 2^57
+                        if (G::idx(0, t, j) < q) {
+                            if constexpr (W) acc = madd(acc, canon(shoup_mul_lazy(rg.x[j], c, cq, P)), P);
+                            else acc += shoup_mul_lazy(rg.x[j], c, cq, P);  // < 2^57
+                        }
                     },
                     [&](auto) CF_INL { pin(acc); });
                 const u64 part = canon(shoup_mul_lazy(acc, 1, misc()[MI_ONEQ], P));
@@ -811,6 +837,9 @@ struct PrimeRun {
                 const u64* Dt = D();
                 const u64 mu = misc()[MI_ONEQ];  // floor(2^64 / p)
                 const u64 fwrap = (t == 0 && n == L) ? mont_pow(gm, (u64)L, m) : 0;
+                // W: the multipliers p of the slots as a running Montgomery form (p = t + j T)
+                u64 pm = W ? to_mont((u64)t, m) : 0;
+                const u64 pmT = W ? to_mont((u64)T, m) : 0, pmL = (W && t == 0 && n == L) ? to_mont((u64)L, m) : 0;
                 pipe_pairs<E, PIPE_D, WIN_K>(
                     [&](auto jc) CF_INL {
                         const int i = G::idx(0, t, decltype(jc)::value), p = i == 0 ? L : i;
@@ -823,14 +852,21 @@ struct PrimeRun {
                         const int p = wrap ? L : i;
                         pin(rg.x[j]);
                         if (p > v && p <= n) {
-                            // p e[p]: with p floor(2^64/p) for the companion the quotient estimate
-                            // loses at most p (x < 8P) / 2^64 < 8 more, so pe < 12P
-                            const u64 pe = shoup_mul_lazy(rg.x[j], (u64)p, (u64)p * mu, P);
-                            const u64 y = shoup_mul_lazy(dv + 12 * P - pe, c, cq, P);
-                            rg.x[j] = mont_mul(y, wrap ? fwrap : f, m);
+                            if constexpr (W) {  // x < 2P and pm < P keep the product exact below 2^126
+                                const u64 pe = mont_mul(rg.x[j], wrap ? pmL : pm, m);  // p e[p], canonical
+                                const u64 y = canon(shoup_mul_lazy(dv + P - pe, c, cq, P));
+                                rg.x[j] = mont_mul(y, wrap ? fwrap : f, m);
+                            } else {
+                                // p e[p]: with p floor(2^64/p) for the companion the quotient estimate
+                                // loses at most p (x < 8P) / 2^64 < 8 more, so pe < 12P
+                                const u64 pe = shoup_mul_lazy(rg.x[j], (u64)p, (u64)p * mu, P);
+                                const u64 y = shoup_mul_lazy(dv + 12 * P - pe, c, cq, P);
+                                rg.x[j] = mont_mul(y, wrap ? fwrap : f, m);
+                            }
                             st_stream(col + p, rg.x[j]);
                         }
                         f = mont_mul(f, step, m);
+                        if constexpr (W) pm = madd(pm, pmT, P);
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
@@ -918,6 +954,7 @@ struct PrimeRun {
                     y = sh(y, inv(), k);
                     y = sh(y, ifact(), nj - k);
                     y = sh(y, ifact(), Mj - k);
+                    if constexpr (W) y = canon(y);  // a factor below 2^62 keeps mont_mul exact
                     y = mont_mul(y, mont_pow(Qm, (u64)(nj - k), m), m);
                     acc = madd(acc, y, P);
                 }

@@ -76,20 +76,28 @@ def lib():
         L.cf_workspace_bytes.restype = ctypes.c_uint64
         L.cf_max_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.cf_max_batch.restype = ctypes.c_long
+        L.cf_prime_range_bits.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_int, _u64p]
+        L.cf_prime_range_bits.restype = ctypes.c_long
+        L.cf_need_bits.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.cf_need_bits.restype = ctypes.c_long
+        L.cf_engine_set_prime_bits.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.cf_engine_set_prime_bits.restype = ctypes.c_int
         L.cf_last_launches.argtypes = [ctypes.c_void_p]
         L.cf_last_launches.restype = ctypes.c_long
         _lib = L
     return _lib
 
 
-def prime_range(first, count):
+def prime_range(first, count, bits=50):
+    """Primes number first .. first+count-1 of the fixed list below 2^bits (bits = 50, or 62 for the
+    list of the reference's -DFP_RB=64 build)."""
     out = np.zeros(max(count, 0), dtype=np.uint64)
-    got = lib().cf_prime_range(first, count, out.ctypes.data_as(_u64p))
+    got = lib().cf_prime_range_bits(first, count, bits, out.ctypes.data_as(_u64p))
     return [int(x) for x in out[:got]]
 
 
-def need(n, M, d, model=MODEL_SUBSET):
-    return int(lib().cf_need(n, M, d, model))
+def need(n, M, d, model=MODEL_SUBSET, bits=50):
+    return int(lib().cf_need_bits(n, M, d, model, bits))
 
 
 def transform_length(nmax):

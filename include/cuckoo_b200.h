@@ -42,6 +42,12 @@ long cf_prime_range(long first, long count, uint64_t* out);
  * Replaces need / log2_Q, fast/cuckoo_fast.cu:452-459 (CF_MODEL_REPLACEMENT: log2 Q = d log2 M). */
 long cf_need(int n, int M, int d, int model);
 
+/* The same two for the list below 2^62 of the reference's -DFP_RB=64 build (PRIME_BITS = 62,
+ * fast/cuckoo_fast.cu:48-57): bits = 50 or 62.  cf_residues accepts primes of either list (it
+ * selects the kernels for primes below 2^62 when a prime is 2^50 or above). */
+long cf_prime_range_bits(long first, long count, int bits, uint64_t* out);
+long cf_need_bits(int n, int M, int d, int model, int bits);
+
 /* max(16, next_pow2(nmax)).  Replaces transform_length, fast/cuckoo_fast.cu:460-472. */
 uint64_t cf_transform_length(uint64_t nmax);
 
@@ -72,7 +78,9 @@ int cf_residues(cf_engine* e, const uint64_t* primes, int B, int nmax, int d, in
                 int J, uint64_t* residues);
 
 /* Same computation with the primes and residues in device memory, enqueued on `stream`
- * (a cudaStream_t; NULL is the CUDA default stream); returns without waiting. */
+ * (a cudaStream_t; NULL is the CUDA default stream); returns without waiting.  The primes are
+ * not read on the host: they must lie below 2^50 unless cf_engine_set_prime_bits(e, 62). */
+int cf_engine_set_prime_bits(cf_engine* e, int bits);
 int cf_residues_async(cf_engine* e, const uint64_t* d_primes, int B, int nmax, int d, int model, const int* qn,
                       const int* qM, int J, uint64_t* d_residues, void* stream);
 

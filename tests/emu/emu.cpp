@@ -67,13 +67,13 @@ struct RFor {
     static constexpr int R = LG >= 10 ? 5 : (LG >= 6 ? LG - 5 : 1);
 };
 
-template <int LG>
+template <int LG, bool W>
 static int run_lg(const KParams& kp) {
     typedef Geo<LG, RFor<LG>::R> G;
     std::vector<u64> smem(Smem<G>::WORDS);
     for (int b = 0; b < kp.B; ++b) {
         HostExec<G> ex;
-        PrimeRun<G, HostExec<G>> pr(ex, kp, b, smem.data());
+        PrimeRun<G, HostExec<G>, W> pr(ex, kp, b, smem.data());
         pr.run();
     }
     return 0;
@@ -136,18 +136,20 @@ static int emu_run(const uint64_t* primes, int B, int nmax, int d, int model, co
         kp.keep = keep->data();
         kp.keep_words = make_keep_layout(nmax, F).total;
     }
+    bool wide = false;  // the kernels for primes below 2^62, as the engine selects them
+    for (int b = 0; b < B; ++b) wide = wide || primes[b] >= (1ull << 50);
     switch (lg) {
-        case 4: run_lg<4>(kp); break;
-        case 5: run_lg<5>(kp); break;
-        case 6: run_lg<6>(kp); break;
-        case 7: run_lg<7>(kp); break;
-        case 8: run_lg<8>(kp); break;
-        case 9: run_lg<9>(kp); break;
-        case 10: run_lg<10>(kp); break;
-        case 11: run_lg<11>(kp); break;
-        case 12: run_lg<12>(kp); break;
-        case 13: run_lg<13>(kp); break;
-        case 14: run_lg<14>(kp); break;
+        case 4: wide ? run_lg<4, true>(kp) : run_lg<4, false>(kp); break;
+        case 5: wide ? run_lg<5, true>(kp) : run_lg<5, false>(kp); break;
+        case 6: wide ? run_lg<6, true>(kp) : run_lg<6, false>(kp); break;
+        case 7: wide ? run_lg<7, true>(kp) : run_lg<7, false>(kp); break;
+        case 8: wide ? run_lg<8, true>(kp) : run_lg<8, false>(kp); break;
+        case 9: wide ? run_lg<9, true>(kp) : run_lg<9, false>(kp); break;
+        case 10: wide ? run_lg<10, true>(kp) : run_lg<10, false>(kp); break;
+        case 11: wide ? run_lg<11, true>(kp) : run_lg<11, false>(kp); break;
+        case 12: wide ? run_lg<12, true>(kp) : run_lg<12, false>(kp); break;
+        case 13: wide ? run_lg<13, true>(kp) : run_lg<13, false>(kp); break;
+        case 14: wide ? run_lg<14, true>(kp) : run_lg<14, false>(kp); break;
         default: return -4;
     }
     return err ? -5 : 0;

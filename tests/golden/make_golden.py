@@ -3,8 +3,8 @@
 
 The fixtures are outputs of the reference (zcy05331/Cuckoo-Failure) built from its sources by
 oracle/Makefile.ref into oracle/_ref/: the 64-bit batch engine's host build
-(fast/cuckoo_fast.cu, byte-identical scalar and AVX-512 IFMA builds) and the 32-bit library CLI
-(src/cuckoo_fail.cpp).  They pin the oracle and the CUDA engine to the reference.
+(fast/cuckoo_fast.cu, byte-identical scalar and AVX-512 IFMA builds, and the scalar build with
+62-bit primes, -DFP_RB=64) and the 32-bit library CLI (src/cuckoo_fail.cpp).  They pin the oracle and the CUDA engine to the reference.
 
 Run from the repository root, where the reference tree is available:
     make -f oracle/Makefile.ref && python tests/golden/make_golden.py
@@ -26,13 +26,13 @@ def fast_bin():
     return ifma if has_ifma and os.path.exists(ifma) else os.path.join(REF, "cuckoo_fast_cpu")
 
 
-def run_fast(d, queries, first, count, out_name, batch=None):
+def run_fast(d, queries, first, count, out_name, batch=None, binary=None):
     """fast/cuckoo_fast.cu CLI: cuckoo_fast D QUERIES FIRST COUNT [--batch B] -> 'i p n M residue' lines."""
     with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
         for n, M in queries:
             f.write(f"{n} {M}\n")
         qpath = f.name
-    cmd = [fast_bin(), str(d), qpath, str(first), str(count)]
+    cmd = [binary or fast_bin(), str(d), qpath, str(first), str(count)]
     if batch:
         cmd += ["--batch", str(batch)]
     out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
@@ -59,6 +59,12 @@ def main():
     # the headline size (n=16384, M=2n) for d = 2, 3, 4, prime 0 (and prime 1 for d = 3)
     for d, cnt in ((2, 1), (3, 2), (4, 1)):
         run_fast(d, [(16384, 32768)], 0, cnt, f"fast_n16384_d{d}.txt")
+
+    # 62-bit primes (-DFP_RB=64): small sizes, config 2, and the headline size for prime 0
+    b64 = os.path.join(REF, "cuckoo_fast_cpu64")
+    run_fast(3, small, 0, 24, "fast62_small_d3.txt", binary=b64)
+    run_fast(2, [(4096, 8192), (1000, 3000)], 0, 2, "fast62_n4096_d2.txt", binary=b64)
+    run_fast(3, [(16384, 32768)], 0, 1, "fast62_n16384_d3.txt", binary=b64)
 
     # 32-bit library CLI: N_bad mod P and exact N_bad (config 1 and the replacement model)
     lines = []

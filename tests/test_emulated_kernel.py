@@ -43,3 +43,23 @@ def test_emulated_kernel_32bit_library_primes():
         if rec[0] == "mod" and rec[2] >= 20:
             _, rep, n, M, d, P, r = rec
             assert h.emu_residues([P], n, d, [(n, M)], rep) == [[r]], rec
+
+
+def test_emulated_kernel_62bit_primes():
+    """Primes below 2^62 select the kernel with [0, 2p) transform values: against the reference's
+    -DFP_RB=64 output and the oracle, both models."""
+    d, queries, first, count, lines = h.load_fast_golden("fast62_small_d3.txt")
+    exp = h.expected_by_prime(lines)
+    items = sorted(exp.items())[:2]
+    qs = [q for q in queries if q[0] <= 300]
+    got = h.emu_residues([p for (i, p), _ in items], 300, d, qs)
+    for ((i, p), want), row in zip(items, got):
+        for q, r in zip(qs, row):
+            if q in want:
+                assert r == want[q], (i, q)
+    import cuckoo_b200 as cb
+
+    for model in (0, 1):
+        ps = cb.prime_range(5, 2, bits=62)
+        for nmax, dd, qq in ((64, 2, [(64, 200), (10, 11)]), (1000, 3, [(1000, 1500)])):
+            assert h.emu_residues(ps, nmax, dd, qq, model) == [h.oracle_residues(p, nmax, dd, qq, model) for p in ps]

@@ -69,3 +69,15 @@ def test_cli_resume_at_prime_boundary(tmp_path):
     assert out.read_text() == want
     r = run_cli(cb.CLI_PATH, d, qpath, first, count, out)
     assert "nothing to do" in r.stderr
+
+
+def test_cli_62bit_identical_to_reference_fp_rb_64(tmp_path):
+    """--prime-bits 62 against the reference built with -DFP_RB=64, byte for byte."""
+    ref_bin = os.path.join(h.ROOT, "oracle", "_ref", "cuckoo_fast_cpu64")
+    if not os.path.exists(ref_bin):
+        pytest.skip("reference -DFP_RB=64 build not available")
+    qpath = write_queries(tmp_path, [(300, 700), (64, 200), (9, 10)])
+    mine = subprocess.run([cb.CLI_PATH, "3", qpath, "0", "30", "--prime-bits", "62"], capture_output=True, text=True)
+    assert mine.returncode == 0, mine.stderr
+    ref = subprocess.run([ref_bin, "3", qpath, "0", "30"], capture_output=True, text=True, check=True)
+    assert mine.stdout == ref.stdout

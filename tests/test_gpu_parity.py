@@ -94,3 +94,17 @@ def test_gpu_rejects_bad_arguments(eng):
         eng.residues([p0], 16385, 3, [(16385, 40000)])
     assert e.value.code == cb.CF_ERR_UNSUPPORTED
     assert eng.residues([], 100, 3, [(100, 200)]).shape == (0, 1)
+
+
+@pytest.mark.parametrize("name", ["fast62_small_d3.txt", "fast62_n4096_d2.txt", "fast62_n16384_d3.txt"])
+def test_gpu_matches_reference_62bit(eng, name):
+    """Primes below 2^62 against the reference built with -DFP_RB=64."""
+    assert check_golden(eng, name) > 0
+
+
+def test_gpu_62bit_mixed_with_oracle(eng):
+    for model in (0, 1):
+        ps = cb.prime_range(40, 3, bits=62)
+        qs = [(777, 2000), (100, 101)]
+        got = eng.residues(ps, 777, 3, qs, model=model)
+        assert [[int(x) for x in r] for r in got] == [h.oracle_residues(p, 777, 3, qs, model) for p in ps]

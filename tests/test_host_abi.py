@@ -52,3 +52,16 @@ def test_workspace_bytes_grows_quadratically():
     # V and S in 16 x 16 blocks at their peak live size, about n^2 / 4 words each
     n = 16384
     assert n * n // 2 * 8 <= cb.workspace_bytes(n, 2 * n, 1) < (n * n // 2 + 2 * 1024 * 1024) * 8
+
+
+def test_62bit_prime_list_and_need_match_reference_output():
+    """cf_prime_range_bits / cf_need_bits with 62 bits reproduce the -DFP_RB=64 reference's output:
+    the same primes, and exactly need(n, M) lines per query."""
+    d, queries, first, count, lines = h.load_fast_golden("fast62_small_d3.txt")
+    primes = sorted({(i, p) for i, p, *_ in lines})
+    assert cb.prime_range(0, count, bits=62) == [p for _, p in primes]
+    assert all(p < 2**62 and p > 2**61 and (p - 1) % 2**20 == 0 for _, p in primes)
+    for n, M in queries:
+        got = sum(1 for ln in lines if (ln[2], ln[3]) == (n, M))
+        assert got == min(count, cb.need(n, M, d, bits=62)), (n, M)
+    assert cb.need(16384, 32768, 3, bits=62) < cb.need(16384, 32768, 3)  # about 20 % fewer primes

@@ -14,7 +14,7 @@ def by_prime(name):
 
 
 @pytest.mark.parametrize("name", ["fast_small_d2.txt", "fast_small_d3.txt", "fast_small_d4.txt",
-                                  "fast_n300_first17.txt", "fast_d1.txt"])
+                                  "fast_n300_first17.txt", "fast_d1.txt", "fast62_small_d3.txt"])
 def test_oracle_matches_reference_fast_engine(name):
     d, queries, exp = by_prime(name)
     nmax = max(n for n, _ in queries)
@@ -94,3 +94,11 @@ def test_oracle_exact_crt_small():
         t = ((r - x) * pow(m, -1, p)) % p
         x, m = x + m * t, m * p
     assert x == nbad
+
+
+def test_oracle_62bit_n4096():
+    """The reference built with -DFP_RB=64 (primes below 2^62, Montgomery R = 2^64)."""
+    d, queries, exp = by_prime("fast62_n4096_d2.txt")
+    for (i, p), want in sorted(exp.items()):
+        qs = sorted(want)
+        assert dict(zip(qs, h.oracle_residues(p, 4096, d, qs))) == want
