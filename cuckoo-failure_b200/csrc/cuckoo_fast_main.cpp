@@ -42,9 +42,12 @@ int main(int argc, char** argv) {
         else if (!std::strcmp(argv[i], "--out") && i + 1 < argc) out_path = argv[++i];
         else if (!std::strcmp(argv[i], "--device") && i + 1 < argc) device = std::atoi(argv[++i]);
         else if (!std::strcmp(argv[i], "--replacement")) model = CF_MODEL_REPLACEMENT;
-        else if (!std::strcmp(argv[i], "--prime-bits") && i + 1 < argc && (bits = std::atoi(argv[++i])) != 50 && bits != 62) {
-            std::fprintf(stderr, "--prime-bits takes 50 or 62\n");
-            return 2;
+        else if (!std::strcmp(argv[i], "--prime-bits") && i + 1 < argc) {
+            bits = std::atoi(argv[++i]);
+            if (bits != 50 && bits != 62) {
+                std::fprintf(stderr, "--prime-bits takes 50 or 62\n");
+                return 2;
+            }
         }
         else {
             std::fprintf(stderr, "unknown option %s\n", argv[i]);

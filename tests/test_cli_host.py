@@ -29,3 +29,14 @@ def test_cli_nothing_to_do_for_complete_file(tmp_path):
     out.write_text("0 1 8 9 5\n1 1 8 9 5\n2 1 8 9 5\n")
     r = run(["3", str(q), "0", "3", "--out", str(out)])
     assert r.returncode == 0 and "nothing to do" in r.stderr
+
+
+def test_cli_rejects_bad_prime_bits(tmp_path):
+    import subprocess
+
+    import cuckoo_b200 as cb
+
+    q = tmp_path / "q.txt"
+    q.write_text("20 40\n")
+    r = subprocess.run([cb.CLI_PATH, "3", str(q), "0", "2", "--prime-bits", "40"], capture_output=True, text=True)
+    assert r.returncode == 2 and "50 or 62" in r.stderr
