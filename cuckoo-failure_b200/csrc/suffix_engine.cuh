@@ -575,6 +575,17 @@ struct PrimeRun {
     // value of a pair table, canonical
     CF_HD static u64 val(const u64* pairs, int k) { return CF_LDG(pairs + 2 * k); }
 
+    // The slots' powers h^(t + jT), j = 0 .. E-1, as NCH independent running products: chain c
+    // holds h^(t + jT) for j = c (mod NCH) and steps by h^(NCH T), so the products that depend on
+    // one another are NCH times fewer than with one chain.
+    static constexpr int NCH = E >= 4 ? 4 : E;
+    CF_HD void power_chains(u64 h, int t, const Mod& m, u64 (&f)[NCH], u64& step) const {
+        f[0] = mont_pow(h, (u64)t, m);
+        const u64 hT = mont_pow(h, (u64)T, m);
+        for (int c = 1; c < NCH; ++c) f[c] = mont_mul(f[c - 1], hT, m);
+        step = mont_pow(hT, (u64)NCH, m);  // h^(NCH T)
+    }
+
     // g(v) and 1/g(v) in Montgomery form (g != 0 for v >= d0)
     CF_HD u64 g_mont(int v, const Mod& m) const {
         if (kp.model == MODEL_REPLACEMENT) return mont_pow(to_mont((u64)v, m), (u64)kp.d, m);
@@ -812,17 +823,16 @@ struct PrimeRun {
             ex.sync();  // column v of S is read below
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const Mod m = md();
-                const u64 gi = ginv_mont(v, m);
-                u64 f = mont_pow(gi, (u64)t, m);           // g^-t
-                const u64 step = mont_pow(gi, (u64)T, m);  // g^-T
+                u64 f[NCH], step;  // g^-(t + jT)
+                power_chains(ginv_mont(v, m), t, m, f, step);
                 // columns q <= d0 of S are zero (stage 1 skipped: row q of V is zero), never written
                 load_row(t, rg.x, S(), SS(), v, d0 + 1, v + 1);
                 window<E, WIN_K>(
                     [&](auto jc) CF_INL {
                         constexpr int j = decltype(jc)::value;
                         pin(rg.x[j]);
-                        rg.x[j] = mont_mul(rg.x[j], f, m);
-                        f = mont_mul(f, step, m);
+                        rg.x[j] = mont_mul(rg.x[j], f[j % NCH], m);
+                        f[j % NCH] = mont_mul(f[j % NCH], step, m);
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
@@ -830,8 +840,8 @@ struct PrimeRun {
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const Mod m = md();
                 const u64 gm = g_mont(v, m);
-                u64 f = mont_pow(gm, (u64)t, m);           // g^t
-                const u64 step = mont_pow(gm, (u64)T, m);  // g^T
+                u64 f[NCH], step;  // g^(t + jT)
+                power_chains(gm, t, m, f, step);
                 const u64 dv = val(D(), v);
                 u64* col = VS() + (size_t)(v - tile_v0(v)) * (n + 1);  // V[.][v], by row
                 const u64* Dt = D();
@@ -855,17 +865,17 @@ struct PrimeRun {
                             if constexpr (W) {  // x < 2P and pm < P keep the product exact below 2^126
                                 const u64 pe = mont_mul(rg.x[j], wrap ? pmL : pm, m);  // p e[p], canonical
                                 const u64 y = canon(shoup_mul_lazy(dv + P - pe, c, cq, P));
-                                rg.x[j] = mont_mul(y, wrap ? fwrap : f, m);
+                                rg.x[j] = mont_mul(y, wrap ? fwrap : f[j % NCH], m);
                             } else {
                                 // p e[p]: with p floor(2^64/p) for the companion the quotient estimate
                                 // loses at most p (x < 8P) / 2^64 < 8 more, so pe < 12P
                                 const u64 pe = shoup_mul_lazy(rg.x[j], (u64)p, (u64)p * mu, P);
                                 const u64 y = shoup_mul_lazy(dv + 12 * P - pe, c, cq, P);
-                                rg.x[j] = mont_mul(y, wrap ? fwrap : f, m);
+                                rg.x[j] = mont_mul(y, wrap ? fwrap : f[j % NCH], m);
                             }
                             st_stream(col + p, rg.x[j]);
                         }
-                        f = mont_mul(f, step, m);
+                        f[j % NCH] = mont_mul(f[j % NCH], step, m);
                         if constexpr (W) pm = madd(pm, pmT, P);
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
