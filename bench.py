@@ -128,9 +128,9 @@ def cpu_baseline(n, M, d):
                       f"{kind}, {dt:.1f} s wall"}
 
 
-def golden_check(n, M, d):
+def golden_check(n, M, d, bits=50):
     """Known residues of the reference host build for primes 0 and 1 (tests/golden)."""
-    path = os.path.join(ROOT, "tests", "golden", f"fast_n{n}_d{d}.txt")
+    path = os.path.join(ROOT, "tests", "golden", f"fast{'62' if bits == 62 else ''}_n{n}_d{d}.txt")
     if not os.path.exists(path):
         return {}
     out = {}
@@ -192,6 +192,8 @@ def main():
     ap.add_argument("--M", type=int, default=32768)
     ap.add_argument("--d", type=int, default=3)
     ap.add_argument("--batch", type=int, default=0, help="primes per step per GPU (default: one wave)")
+    ap.add_argument("--prime-bits", type=int, default=50, choices=[50, 62],
+                    help="prime list: below 2^50 (default) or below 2^62 (the reference's -DFP_RB=64 build)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-query latency run")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
@@ -203,7 +205,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    workload = f"one-table suffix build + nbad query, n={n}, M={M}, d={d}, 50-bit primes of the fixed list"
+    workload = f"one-table suffix build + nbad query, n={n}, M={M}, d={d}, {a.prime_bits}-bit primes of the fixed list"
 
     if a.impl == "reference":
         if rank != 0:
@@ -251,7 +253,10 @@ def main():
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     # one wave, one prime below what fits now: what the launch sees must still hold the whole batch
     B = a.batch or max(1, min(eng.max_batch(n, M, J) - 1, sms))
-    primes = cb.prime_range(rank * B, B)
+    primes = cb.prime_range(rank * B, B, bits=a.prime_bits)
+    if a.prime_bits != 50:
+        lib_rc = cb.lib().cf_engine_set_prime_bits(eng._h, a.prime_bits)
+        assert lib_rc == 0
     stream = torch.cuda.Stream()  # a dedicated stream: the events below are recorded on it
     d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
     d_out = torch.empty(B * J, dtype=torch.int64, device="cuda")
@@ -264,7 +269,7 @@ def main():
     torch.cuda.synchronize()
     # self-check against the reference's residues for the primes it covers
     got = d_out.cpu().numpy().view(np.uint64)
-    for i, r in golden_check(n, M, d).items():
+    for i, r in golden_check(n, M, d, a.prime_bits).items():
         if rank == 0 and i < B:
             assert int(got[i]) == r, f"residue mismatch at prime {i}: {int(got[i])} != {r}"
 
