@@ -31,7 +31,7 @@ UNIT = "prime-residues/s"
 K_OPS_PER_MM = 20  # INT32 multiply ops per 64-bit modular multiplication (fixed accounting model)
 # DRAM bytes (read + write) per launch of the engine kernel, from the ncu launch list of this
 # bench's own command (profiles/k_suffix_n16384_b148_launches.md), keyed by (n, M, d, primes per launch)
-MEASURED_TRAFFIC = {(16384, 32768, 3, 148): 976.4e9 + 638.9e9}
+MEASURED_TRAFFIC = {(16384, 32768, 3, 148): 997.6e9 + 639.0e9}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 
