@@ -88,8 +88,17 @@ struct DevExec {
     }
 };
 
+// Resident CTAs per SM the kernel is compiled for (registers per thread <= 65536 / (T x this)).
+// Measured on B200 (prime-residues/s, the same batch per SM, n = 2^LG):
+//   L = 2^10 (32 threads): 1 -> 6.9k, 12 -> 7.3k, 16 (128 registers, ptxas -O1) -> 8.9k: 16;
+//   L = 2^11 .. 2^13: capping registers (1 -> 4/6/8 CTAs) lost 2 .. 20 %: 1 (no cap);
+//   L = 2^14: one CTA per SM is forced by its shared memory and tensor memory anyway.
+template <int LG>
+struct MinBlocks {
+    static constexpr int v = LG == 10 ? 16 : 1;
+};
 template <int LG, int R, bool W>
-__global__ void __launch_bounds__(Geo<LG, R>::T) k_suffix(KParams kp) {
+__global__ void __launch_bounds__(Geo<LG, R>::T, MinBlocks<LG>::v) k_suffix(KParams kp) {
     typedef Geo<LG, R> G;
     extern __shared__ __align__(16) u64 smem[];
     DevExec<G> ex;
