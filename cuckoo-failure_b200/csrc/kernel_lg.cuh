@@ -91,7 +91,7 @@ struct DevExec {
 // Resident CTAs per SM the kernel is compiled for (registers per thread <= 65536 / (T x this)).
 // Measured on B200 (prime-residues/s, the same batch per SM, n = 2^LG):
 //   L = 2^10 (32 threads): 1 -> 6.9k, 12 -> 7.3k, 16 (128 registers, ptxas -O1) -> 8.9k: 16;
-//   L = 2^11 .. 2^13: capping registers (1 -> 4/6/8 CTAs) lost 2 .. 20 %: 1 (no cap);
+//   L = 2^11 .. 2^13 (then with 32 entries per thread): capping registers lost 2 .. 20 %: 1 (no cap);
 //   L = 2^14: one CTA per SM is forced by its shared memory and tensor memory anyway.
 template <int LG>
 struct MinBlocks {
@@ -106,11 +106,13 @@ __global__ void __launch_bounds__(Geo<LG, R>::T, MinBlocks<LG>::v) k_suffix(KPar
     pr.run();
 }
 
-// Elements per thread: 32 for L >= 1024 (one register pass per 5 levels), fewer below so a CTA
-// keeps at least a few warps' worth of threads.
+// Elements per thread (2^R): 32 at L = 2^10 and 2^14, 16 at L = 2^11 .. 2^13, fewer below so a CTA
+// keeps at least a warp.  R = 4 at 2^11 .. 2^13 was measured on B200 against R = 5 (twice the
+// threads, about 165 registers each): n = 2048: 1826 -> 2244, n = 4096: 496 -> 540, n = 8192:
+// 122 -> 170 prime-residues/s.  At 2^14, R = 5 keeps 512 threads (the tensor-memory layout).
 template <int LG>
 struct RFor {
-    static constexpr int R = LG >= 10 ? 5 : (LG >= 6 ? LG - 5 : 1);
+    static constexpr int R = (LG >= 11 && LG <= 13) ? 4 : (LG >= 10 ? 5 : (LG >= 6 ? LG - 5 : 1));
 };
 
 typedef void (*kfn_t)(KParams);

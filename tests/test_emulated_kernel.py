@@ -18,11 +18,14 @@ def test_emulated_kernel_matches_oracle(nmax, d, queries, model):
     assert h.emu_residues([P0], nmax, d, queries, model)[0] == h.oracle_residues(P0, nmax, d, queries, model)
 
 
-def test_emulated_kernel_r5_geometry():
-    """L = 1024 and 2048: five-level register passes (the geometry of the large transforms)."""
+def test_emulated_kernel_large_geometries():
+    """L = 1024 (32 entries per thread, five-level register passes, as at 2^14) and L = 2048
+    (16 entries per thread, four-level passes, as at 2^11 .. 2^13)."""
     ps = h.oracle_primes(0, 2)
     for nmax, d, qs in ((1000, 3, [(1000, 2000), (999, 1001)]), (1024, 2, [(1024, 3000), (7, 9)])):
         assert h.emu_residues(ps, nmax, d, qs) == [h.oracle_residues(p, nmax, d, qs) for p in ps]
+    p = ps[1]
+    assert h.emu_residues([p], 1500, 3, [(1500, 4000), (800, 801)]) == [h.oracle_residues(p, 1500, 3, [(1500, 4000), (800, 801)])]
 
 
 def test_emulated_kernel_golden_small():
