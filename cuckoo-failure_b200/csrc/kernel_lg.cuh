@@ -24,7 +24,7 @@ struct DevExec {
     __device__ __forceinline__ void sync() { __syncthreads(); }
     __device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
     // Tensor memory: one warp allocates all 512 columns for the CTA (one CTA per SM uses it);
-    // thread t of warp w owns lane 32 (w % 4) + (t % 32), columns 128 (w / 4) + [0, 128).
+    // thread t of warp w owns lane 32 (w % 4) + (t % 32), columns 4E (w / 4) + [0, 4E): E pairs.
     __device__ __forceinline__ void tmem_alloc(u32* slot) {
         if ((threadIdx.x >> 5) == 0) {
             asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -44,7 +44,7 @@ struct DevExec {
     }
     __device__ __forceinline__ static u32 tmem_addr(u32 base, int t) {
         const int w = t >> 5;
-        return base + ((u32)(32 * (w & 3)) << 16) + (u32)(128 * (w >> 2));
+        return base + ((u32)(32 * (w & 3)) << 16) + (u32)(4 * G::E * (w >> 2));
     }
     __device__ __forceinline__ void tmem_st16(int, u32 ta, const u32 (&v)[16]) {
         asm volatile(
@@ -106,13 +106,13 @@ __global__ void __launch_bounds__(Geo<LG, R>::T, MinBlocks<LG>::v) k_suffix(KPar
     pr.run();
 }
 
-// Elements per thread (2^R): 32 at L = 2^10 and 2^14, 16 at L = 2^11 .. 2^13, fewer below so a CTA
-// keeps at least a warp.  R = 4 at 2^11 .. 2^13 was measured on B200 against R = 5 (twice the
-// threads, about 165 registers each): n = 2048: 1826 -> 2244, n = 4096: 496 -> 540, n = 8192:
-// 122 -> 170 prime-residues/s.  At 2^14, R = 5 keeps 512 threads (the tensor-memory layout).
+// Elements per thread (2^R): 32 at L = 2^10, 16 at L = 2^11 .. 2^14, fewer below so a CTA keeps at
+// least a warp.  R = 4 was measured on B200 against R = 5 (twice the threads): n = 2048: 1826 ->
+// 2244, n = 4096: 496 -> 540, n = 8192: 122 -> 170, n = 16384: 40.8 -> 48.5 prime-residues/s
+// (1024 threads of 64 registers; 32 warps per SM hide the L2 latency of the per-step constants).
 template <int LG>
 struct RFor {
-    static constexpr int R = (LG >= 11 && LG <= 13) ? 4 : (LG >= 10 ? 5 : (LG >= 6 ? LG - 5 : 1));
+    static constexpr int R = (LG >= 11 && LG <= 14) ? 4 : (LG >= 10 ? 5 : (LG >= 6 ? LG - 5 : 1));
 };
 
 typedef void (*kfn_t)(KParams);

@@ -286,9 +286,13 @@ struct Regs {
 template <class G, class X, bool W = false>
 struct PrimeRun {
     static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP, NW = G::NW;
-    // L = 2^14 (512 threads x 32 entries): the kernel spectrum lives in tensor memory, each thread's
-    // 32 (value, companion) pairs in its own 128 columns; smaller transforms read it from global.
-    static constexpr bool TM = (T == 512 && E == 32);
+    // L = 2^14 (1024 threads x 16 entries): the kernel spectrum lives in tensor memory, each
+    // thread's 16 (value, companion) pairs in its own 64 columns (all 512 columns of the SM's 128
+    // lanes); smaller transforms, several CTAs to an SM, read it from global.
+    static constexpr bool TM = (T == 1024 && E == 16) || (T == 512 && E == 32);
+    // Constants in flight and units in flight of the hot loops.  At 1024 threads (64 registers each)
+    // the shallowest schedule spills least and measured fastest (49.7 vs 48.9 prime-residues/s).
+    static constexpr int PD = T >= 1024 ? 1 : PIPE_D, WK = T >= 1024 ? 1 : WIN_K;
     X& ex;
     const KParams& kp;
     int b;      // prime index within the batch
@@ -386,7 +390,7 @@ struct PrimeRun {
     template <int PASS, bool FWD>
     CF_HD void pass(int t, u64 (&x)[E]) const {
         typedef Plan<PASS, FWD> PL;
-        constexpr int D = PIPE_D;
+        constexpr int D = PD;
         const int off = PL::bb ? (t & ((1 << PL::bb) - 1)) : 0;
         const u64 P4 = 4 * P, P2 = 2 * P;
         u64 rw[D + 1], rq[D + 1];
@@ -394,7 +398,7 @@ struct PrimeRun {
             constexpr int f = decltype(fc)::value;
             if constexpr (f < PL::NG && !PL::trivial_grp(f)) ld_tw<PASS>(tw_addr<PASS, FWD, f>(off), rw[f], rq[f]);
         }, [&](auto) CF_INL {});
-        window<PL::NB, WIN_K>(
+        window<PL::NB, WK>(
             [&](auto qc) CF_INL {
                 constexpr int q = decltype(qc)::value, f = PL::grp(q), fn = f + D;
                 if constexpr (PL::kk(q) == 0 && fn < PL::NG && !PL::trivial_grp(fn))
@@ -511,7 +515,7 @@ struct PrimeRun {
             return;
         }
         const u64* h = hat();
-        pipe_pairs<E, PIPE_D, WIN_K>(
+        pipe_pairs<E, PD, WK>(
             [&](auto jc) CF_INL { return h + 2 * G::idx(NP - 1, t, decltype(jc)::value); },
             [&](auto jc, u64 w, u64 wq) CF_INL {
                 constexpr int j = decltype(jc)::value;
@@ -772,7 +776,7 @@ struct PrimeRun {
                 const u64* iv = inv();
                 u64 acc = 0;
                 // 1/(M - w) for the slots' w (clamped to a valid entry outside the row)
-                pipe_pairs<E, PIPE_D, WIN_K>(
+                pipe_pairs<E, PD, WK>(
                     [&](auto jc) CF_INL {
                         const int w = G::idx(0, t, decltype(jc)::value);
                         return iv + 2 * (w < q ? Mj - w : Mj);
@@ -804,7 +808,7 @@ struct PrimeRun {
                 const u64 iv = val(inv(), v), ivq = CF_LDG(inv() + 2 * v + 1);
                 u64* col = SS() + (size_t)(v - tile_v0(v)) * (n + 1);  // S[.][v], by row
                 const u64* Dt = D();
-                pipe_pairs<E, PIPE_D, WIN_K>(
+                pipe_pairs<E, PD, WK>(
                     [&](auto jc) CF_INL {
                         const int i = G::idx(0, t, decltype(jc)::value);
                         return Dt + 2 * (i >= v && i < n ? i - v : 0);
@@ -827,7 +831,7 @@ struct PrimeRun {
                 power_chains(ginv_mont(v, m), t, m, f, step);
                 // columns q <= d0 of S are zero (stage 1 skipped: row q of V is zero), never written
                 load_row(t, rg.x, S(), SS(), v, d0 + 1, v + 1);
-                window<E, WIN_K>(
+                window<E, WK>(
                     [&](auto jc) CF_INL {
                         constexpr int j = decltype(jc)::value;
                         pin(rg.x[j]);
@@ -850,7 +854,7 @@ struct PrimeRun {
                 // W: the multipliers p of the slots as a running Montgomery form (p = t + j T)
                 u64 pm = W ? to_mont((u64)t, m) : 0;
                 const u64 pmT = W ? to_mont((u64)T, m) : 0, pmL = (W && t == 0 && n == L) ? to_mont((u64)L, m) : 0;
-                pipe_pairs<E, PIPE_D, WIN_K>(
+                pipe_pairs<E, PD, WK>(
                     [&](auto jc) CF_INL {
                         const int i = G::idx(0, t, decltype(jc)::value), p = i == 0 ? L : i;
                         return Dt + 2 * (p > v && p <= n ? p - v - 1 : 0);

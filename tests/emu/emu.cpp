@@ -35,7 +35,7 @@ struct HostExec {
     void tmem_sync() {}
     static u32 tmem_addr(u32 base, int t) {
         const int w = t >> 5;
-        return base + ((u32)(32 * (w & 3)) << 16) + (u32)(128 * (w >> 2));
+        return base + ((u32)(32 * (w & 3)) << 16) + (u32)(4 * G::E * (w >> 2));
     }
     u32* tmem_word(int t, u32 ta, int k) {
         const int lane = (int)(ta >> 16) + (t & 31), col = (int)(ta & 0xFFFF) + k;
@@ -64,7 +64,7 @@ struct HostExec {
 
 template <int LG>
 struct RFor {
-    static constexpr int R = (LG >= 11 && LG <= 13) ? 4 : (LG >= 10 ? 5 : (LG >= 6 ? LG - 5 : 1));
+    static constexpr int R = (LG >= 11 && LG <= 14) ? 4 : (LG >= 10 ? 5 : (LG >= 6 ? LG - 5 : 1));
 };
 
 template <int LG, bool W>
@@ -110,7 +110,7 @@ static int emu_run(const uint64_t* primes, int B, int nmax, int d, int model, co
     const int L = (int)cfh::transform_length((uint64_t)nmax);
     int lg = 0;
     while ((1 << lg) < L) ++lg;
-    const int R = (lg >= 11 && lg <= 13) ? 4 : (lg >= 10 ? 5 : (lg >= 6 ? lg - 5 : 1)), T = 1 << (lg - R);
+    const int R = (lg >= 11 && lg <= 14) ? 4 : (lg >= 10 ? 5 : (lg >= 6 ? lg - 5 : 1)), T = 1 << (lg - R);
     const Layout lo = make_layout(nmax, F, L, J, T >= 32 ? T / 32 : 1, R);
     // poisoned, like reused device memory: every word the kernel reads must have been written first
     std::vector<u64> ws(lo.total * (size_t)B, 0xA5A5A5A5A5A5A5A5ull);
