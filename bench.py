@@ -30,8 +30,9 @@ METRIC = "prime-residues/s, n=16384 d=3 NTT suffix build; served-query p50/p99 l
 UNIT = "prime-residues/s"
 K_OPS_PER_MM = 20  # INT32 multiply ops per 64-bit modular multiplication (fixed accounting model)
 # DRAM bytes (read + write) per launch of the engine kernel, from the ncu launch list of this
-# bench's own command (profiles/k_suffix_n16384_b148_launches.md), keyed by (n, M, d, primes per launch)
-MEASURED_TRAFFIC = {(16384, 32768, 3, 148): 997.6e9 + 639.0e9}
+# bench's own command (profiles/k_suffix_n16384_b148_launches.md), keyed by (n, M, d, primes per
+# launch, prime bits)
+MEASURED_TRAFFIC = {(16384, 32768, 3, 148, 50): 1390.6e9 + 944.9e9}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 
@@ -330,7 +331,7 @@ def main():
                        "l2": "inputs larger than L2 (per-prime tables total far above 126 MB)"},
             "roofline": {"bound": "int32", "achieved": achieved, "peak": peak, "unit": "Top/s (INT32 IMAD)",
                          "frac": achieved / peak if peak else None,
-                         "traffic": a.traffic_bytes or MEASURED_TRAFFIC.get((n, M, d, B)),
+                         "traffic": a.traffic_bytes or MEASURED_TRAFFIC.get((n, M, d, B, a.prime_bits)),
                          "model": f"{K_OPS_PER_MM} INT32 multiply ops per modular multiplication, "
                                   f"{algorithmic_mm(n):.3e} multiplications per prime-residue; peak measured live"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),

@@ -25,10 +25,10 @@ PROBE_SRC = os.path.join(PKG, "probe", "imad_peak.cu")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
-# Per-unit assembler options.  The L = 2^14 kernel runs 512 threads, so it has 128 registers per
-# thread; at the default level ptxas schedules its transform passes past that budget and spills
-# (a 368-byte stack frame whose traffic goes to L2 when 148 CTAs run), while -O1 fits them in
-# registers.  The L = 2^10 kernel is compiled for 16 CTAs per SM (MinBlocks in kernel_lg.cuh), also
+# Per-unit assembler options.  The L = 2^14 kernel runs 1024 threads, so it has 64 registers per
+# thread; at the default level ptxas schedules its transform passes far past that budget (frames
+# above 800 bytes), while -O1 keeps the 50-bit kernel to a 152-byte frame and the 62-bit one to
+# 320 bytes.  The L = 2^10 kernel is compiled for 16 CTAs per SM (MinBlocks in kernel_lg.cuh), also
 # 128 registers: -O1 keeps it to a 208-byte frame where the default level spills 1.4 KB.  The other
 # kernels have up to 255 registers and spill at neither level.
 UNIT_FLAGS = {"k_lg14.cu": ["-Xptxas", "-O1"], "k_lg10.cu": ["-Xptxas", "-O1"]}
