@@ -112,11 +112,18 @@ CF_HD u64 shoup_companion(u64 w, u64 p) {
 // a w mod p in [0, 4p) for any 64-bit a, given w < p and wq = floor(w 2^64 / p).  The quotient
 // estimate keeps only the partial products of a wq that reach the high word (a1 q1 and the high
 // halves of a0 q1, a1 q0): it is at most 2 below floor(a wq / 2^64), which in turn is at most 1
-// below floor(a w / p), so the remainder lies in [0, 4p).  3 wide + 2 high + 4 low multiplies.
+// below floor(a w / p), so the remainder lies in [0, 4p).  5 wide + 4 low multiplies.
+//
+// On sm_100a a 32 x 32 -> high-32 multiply (mul.hi.u32) issues at under half the rate of a
+// 32 x 32 -> 64 one (mul.wide.u32: 27 against 58 per SM per clock, measured), so the two high
+// halves of the quotient estimate are taken from wide products.
 CF_HD u64 shoup_mul_lazy(u64 a, u64 w, u64 wq, u64 p) {
     const u32 a0 = lo32(a), a1 = hi32(a), q0 = lo32(wq), q1 = hi32(wq);
 #if defined(__CUDA_ARCH__)
-    const u64 q = wmul(a1, q1) + (u64)__umulhi(a0, q1) + (u64)__umulhi(a1, q0);
+    u64 t1, t2, q;
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(t1) : "r"(a0), "r"(q1));
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(t2) : "r"(a1), "r"(q0));
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(q) : "r"(a1), "r"(q1), "l"((t1 >> 32) + (t2 >> 32)));
 #else
     const u64 q = wmul(a1, q1) + (wmul(a0, q1) >> 32) + (wmul(a1, q0) >> 32);
 #endif

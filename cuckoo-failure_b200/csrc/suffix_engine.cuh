@@ -18,7 +18,7 @@
 //       stage 2:  Vs[p][v]  = g^p D[p-v-1] (D[v] - p conv(Ss[v][q] g^-q)[p])
 //       query:    out(q)    = (q-1)! sum_w Vs[q][w] / (M - w)
 //   * the powers g^p and g^-q of a step are running Montgomery products per thread (each thread
-//     holds the entries t + k T), so no per-step tables are built;
+//     holds the entries t + k T), started from a small per-step table of powers in shared memory;
 //   * the queries are evaluated on the fly from the stage-1 input rows (the same U[w] the
 //     reference's k_query builds), reduced per warp and stored per warp, so a batch needs no
 //     separate pass over V and no block barrier per row.
@@ -268,7 +268,10 @@ struct Smem {
     static constexpr int MISC = RED + 2 * G::T + 64;  // [16] modulus constants and scalars
     static constexpr int TWS = MISC + 16;             // pairs w^(k 2^R), k = 0 .. L/2^(R+1): passes >= 1
     static constexpr int TWS_N = (G::L >> (G::R + 1)) + 1;
-    static constexpr int WORDS = TWS + 2 * TWS_N;
+    // [2][PW_STRIDE] powers of 1/g(v) and g(v) for stage 2, rebuilt every step (power_tables)
+    static constexpr int PW = TWS + 2 * TWS_N;
+    static constexpr int PW_STRIDE = 72;
+    static constexpr int WORDS = PW + 2 * PW_STRIDE;
     static constexpr size_t BYTES = (size_t)WORDS * 8;
 };
 enum { MI_P = 0, MI_PINV = 1, MI_R1 = 2, MI_R2 = 3, MI_ONEQ = 4, MI_ROOT = 5, MI_LINV = 6, MI_TMEM = 7 };
@@ -583,11 +586,41 @@ struct PrimeRun {
     // holds h^(t + jT) for j = c (mod NCH) and steps by h^(NCH T), so the products that depend on
     // one another are NCH times fewer than with one chain.
     static constexpr int NCH = E >= 4 ? 4 : E;
-    CF_HD void power_chains(u64 h, int t, const Mod& m, u64 (&f)[NCH], u64& step) const {
-        f[0] = mont_pow(h, (u64)t, m);
-        const u64 hT = mont_pow(h, (u64)T, m);
+
+    // Stage-2 powers of h = 1/g(v) (row load) and h = g(v) (products), Montgomery form.  Rather
+    // than an exponentiation per thread, the CTA builds at the start of each step a two-level
+    // table per base in shared memory: A[k] = h^k (k < TA = min(T, 32)) at slots 0.., B[k] =
+    // h^(TA k) (k < TB = T / TA) at slots 32.., and h^T, h^(NCH T), h^L at slots 64, 65, 66.
+    // Thread t then starts its chains from A[t % TA] B[t / TA].  The 2 (TA + TB + 3) entries are
+    // independent exponentiations; task k runs on lane k / NW of warp k % NW, so every warp takes
+    // a few and none lags at the next barrier.
+    static constexpr int TA = T < 32 ? T : 32, TB = T / TA;
+    static constexpr int PW_TASKS = 2 * (TA + TB + 3);
+    CF_HD void power_tables(int v) {
+        u64* pw = sm + Smem<G>::PW;
+        ex.each([&](int t, Regs<G>&) CF_INL {
+            const Mod m = md();
+            for (int k = (t & 31) * NW + (t >> 5); k < PW_TASKS; k += T) {
+                const int base = k < PW_TASKS / 2 ? 0 : 1, r = k - base * (PW_TASKS / 2);
+                const u64 h = base ? g_mont(v, m) : ginv_mont(v, m);
+                u64 e;
+                int slot;
+                if (r < TA) e = (u64)r, slot = r;
+                else if (r < TA + TB) e = (u64)TA * (r - TA), slot = 32 + r - TA;
+                else if (r == TA + TB) e = (u64)T, slot = 64;
+                else if (r == TA + TB + 1) e = (u64)NCH * T, slot = 65;
+                else e = (u64)L, slot = 66;
+                pw[base * Smem<G>::PW_STRIDE + slot] = mont_pow(h, e, m);
+            }
+        });
+    }
+    // chain c of thread t holds h^(t + jT) for j = c (mod NCH) and steps by h^(NCH T)
+    CF_HD void power_chains(int base, int t, const Mod& m, u64 (&f)[NCH], u64& step) const {
+        const u64* pw = sm + Smem<G>::PW + base * Smem<G>::PW_STRIDE;
+        f[0] = TB > 1 ? mont_mul(pw[t % TA], pw[32 + t / TA], m) : pw[t];
+        const u64 hT = pw[64];
         for (int c = 1; c < NCH; ++c) f[c] = mont_mul(f[c - 1], hT, m);
-        step = mont_pow(hT, (u64)NCH, m);  // h^(NCH T)
+        step = pw[65];
     }
 
     // g(v) and 1/g(v) in Montgomery form (g != 0 for v >= d0)
@@ -798,6 +831,7 @@ struct PrimeRun {
     // One step of the suffix recurrence (fast/cuckoo_fast.cu:841-855).
     CF_HD void step(int v) {
         const int n = kp.n, d0 = kp.d0;
+        if (v >= d0) power_tables(v);  // read after the barriers of stage 1 / the stage-2 barrier
         if (v > d0) {  // stage 1: column v of S from row v of V
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 load_row(t, rg.x, V(), VS(), v, d0, v);  // columns w < d0 of V are zero (g(w) = 0), never written
@@ -828,7 +862,7 @@ struct PrimeRun {
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const Mod m = md();
                 u64 f[NCH], step;  // g^-(t + jT)
-                power_chains(ginv_mont(v, m), t, m, f, step);
+                power_chains(0, t, m, f, step);
                 // columns q <= d0 of S are zero (stage 1 skipped: row q of V is zero), never written
                 load_row(t, rg.x, S(), SS(), v, d0 + 1, v + 1);
                 window<E, WK>(
@@ -843,14 +877,13 @@ struct PrimeRun {
             convolve();
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const Mod m = md();
-                const u64 gm = g_mont(v, m);
                 u64 f[NCH], step;  // g^(t + jT)
-                power_chains(gm, t, m, f, step);
+                power_chains(1, t, m, f, step);
                 const u64 dv = val(D(), v);
                 u64* col = VS() + (size_t)(v - tile_v0(v)) * (n + 1);  // V[.][v], by row
                 const u64* Dt = D();
                 const u64 mu = misc()[MI_ONEQ];  // floor(2^64 / p)
-                const u64 fwrap = (t == 0 && n == L) ? mont_pow(gm, (u64)L, m) : 0;
+                const u64 fwrap = sm[Smem<G>::PW + Smem<G>::PW_STRIDE + 66];  // g^L, for e[n] at index 0 when L = n
                 // W: the multipliers p of the slots as a running Montgomery form (p = t + j T)
                 u64 pm = W ? to_mont((u64)t, m) : 0;
                 const u64 pmT = W ? to_mont((u64)T, m) : 0, pmL = (W && t == 0 && n == L) ? to_mont((u64)L, m) : 0;
