@@ -9,7 +9,8 @@
 // Design (B200, one CTA per prime, persistent over all steps v = 1 .. n-1):
 //   * the length-L transform lives in shared memory between radix-2^R register passes;
 //   * every multiplication by a stored constant is a Shoup product with a precomputed companion;
-//     inside the transforms values stay lazily reduced ([0, 4p) forward, [0, 8p) inverse);
+//     inside the transforms only the twiddle products are reduced (lazily, to [0, 4p)); the sums
+//     grow within the 14 spare bits of a word under bounds tracked per level (Geo);
 //   * the stage factors are folded into what is stored, so stage 1 needs no multiply on input:
 //       Vs[p][w] = V[p][w] / (w! (p-1-w)! (p-1)!)        (stored V)
 //       Ss[v][q] = S[v][q] / (q! (v-q)! v!)              (stored S)
@@ -154,6 +155,16 @@ struct Geo {
         return ((t >> b) << (b + R)) + (t & ((1 << b) - 1)) + (j << b);
     }
     CF_HD static int swz(int i) { return i ^ ((i >> SWZ) & 15); }
+    // Value bounds of the transforms for primes below 2^50 (multiples of p, strict upper bounds),
+    // by level s in processing order.  Forward: canonical inputs, no reduction of sums, so the
+    // inputs of level s lie below 2^s p (2^LG p < 2^64 needs LG <= 14).  Inverse: inputs below 4p;
+    // a butterfly with a twiddle adds a product below 4p, a trivial one (first pass, twiddle 1)
+    // doubles, so no reduction is needed either.
+    static constexpr int R_LAST = LG - (NP - 1) * R;  // levels of the last pass (the trivial groups)
+    CF_HD static constexpr u64 inv_bound(int s) {
+        return s <= R_LAST ? (u64)4 << s : ((u64)4 << R_LAST) + 4 * (u64)(s - R_LAST);
+    }
+    static constexpr u64 INV_OUT = inv_bound(LG);  // bound of the inverse transform's outputs
 };
 
 CF_HD u64 red2(u64 x, u64 m) { return x >= m ? x - m : x; }  // [0, 2m) -> [0, m)
@@ -281,14 +292,15 @@ struct Regs {
     u64 x[G::E];
 };
 
-// W = false: primes below 2^50 (the fixed list of fast/cuckoo_fast.cu with FP_RB = 52); transform
-// values stay lazily reduced in [0, 4p) forward and [0, 8p) inverse.
+// W = false: primes below 2^50 (the fixed list of fast/cuckoo_fast.cu with FP_RB = 52); the
+// transforms reduce only their twiddle products (bounds per level in Geo).
 // W = true: primes below 2^62 (the list of the FP_RB = 64 build); with 8p beyond 2^64 every
 // transform value stays in [0, 2p) instead (one more conditional subtraction per output), and the
 // few products whose lazy factor could reach 2^62 take a canonical one.
 template <class G, class X, bool W = false>
 struct PrimeRun {
     static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP, NW = G::NW;
+    static_assert(W || G::LG <= 14, "reduction-free forward transform needs 2^LG p < 2^64");
     // L = 2^14 (1024 threads x 16 entries): the kernel spectrum lives in tensor memory, each
     // thread's 16 (value, companion) pairs in its own 64 columns (all 512 columns of the SM's 128
     // lanes); smaller transforms, several CTAs to an SM, read it from global.
@@ -342,8 +354,17 @@ struct PrimeRun {
     // Cooley-Tukey with inverse roots (bit-reversed in, natural out, unscaled), the same pair of
     // transforms as fast/cuckoo_fast.cu:258-305 and include/cuckoo/ntt.hpp:97-123.  W[k] = w^k
     // for k <= L/2 (W[L/2] = -1), so w_{2h}^{-j} = -W[L/2 - j L/2h] for every j, including 0.
-    // Forward values stay in [0, 4p), inverse values in [0, 8p).
+    // Primes below 2^50: the transforms reduce nothing but the twiddle products (bounds in Geo);
+    // primes below 2^62: every value stays in [0, 2p).
     // ---------------------------------------------------------------------------------------
+    // Host builds with CF_CHECK_BOUNDS (the CPU harness) verify every bound the transforms rely on.
+    CF_HD void check_bound(u64 x, u64 mult) const {
+#if defined(CF_CHECK_BOUNDS) && !defined(__CUDA_ARCH__)
+        if (x >= mult * P) throw std::runtime_error("transform value above its bound");
+#else
+        (void)x, (void)mult;
+#endif
+    }
     // Butterfly schedule of one register pass.  Unit q runs in order of level (forward: m = r-1
     // down to 0; inverse: 0 up), then twiddle group (ul), then register pair; grp(q) numbers the
     // twiddle groups in that order.
@@ -351,6 +372,9 @@ struct PrimeRun {
     struct Plan {
         static constexpr int bb = G::pass_b(PASS), r = G::pass_r(PASS);
         static constexpr int BPL = E / 2, NB = BPL * r, NG = (1 << r) - 1;
+        // levels done before this pass, in processing order (forward: passes 0 ..; inverse: NP-1 ..)
+        static constexpr int s0 = FWD ? PASS * G::R : (PASS == NP - 1 ? 0 : G::R_LAST + (NP - 2 - PASS) * G::R);
+        CF_HD static constexpr int lvl(int q) { return s0 + q / BPL; }
         CF_HD static constexpr int m(int q) { return FWD ? r - 1 - q / BPL : q / BPL; }
         CF_HD static constexpr int per(int q) { return E >> (m(q) + 1); }  // butterflies per group
         CF_HD static constexpr int ul(int q) { return (q % BPL) / per(q); }
@@ -427,22 +451,28 @@ struct PrimeRun {
                         x[j0] = red2(a - c + P2, P2);
                         x[j1] = red2(a + c, P2);
                     }
-                } else if constexpr (FWD) {
+                } else if constexpr (FWD) {  // inputs below 2^s p, outputs below 2^(s+1) p
+                    constexpr int s = PL::lvl(q);
                     const u64 a = x[j0], c = x[j1];
-                    x[j0] = red2(a + c, P4);
-                    const u64 dd = a - c + P4;
-                    x[j1] = trivial ? red2(dd, P4) : shoup_mul_lazy(dd, w, wq, P);
-                } else {
-                    const u64 a = red2(x[j0], P4);
+                    x[j0] = a + c;
+                    const u64 dd = a - c + (P << s);
+                    if constexpr (trivial) x[j1] = dd;
+                    else if constexpr (s == 0) x[j1] = red2(shoup_mul_lazy(dd, w, wq, P), P2);
+                    else x[j1] = shoup_mul_lazy(dd, w, wq, P);
+                    check_bound(x[j0], (u64)2 << s), check_bound(x[j1], (u64)2 << s);
+                } else {  // inputs below inv_bound(s) p
+                    constexpr int s = PL::lvl(q);
+                    const u64 a = x[j0];
                     if constexpr (trivial) {
-                        const u64 c = red2(x[j1], P4);
+                        const u64 c = x[j1];
                         x[j0] = a + c;
-                        x[j1] = a - c + P4;
+                        x[j1] = a - c + P * G::inv_bound(s);
                     } else {
                         const u64 c = shoup_mul_lazy(x[j1], w, wq, P);  // -w_{2h}^{-j} y
                         x[j0] = a - c + P4;
                         x[j1] = a + c;
                     }
+                    check_bound(x[j0], G::inv_bound(s + 1)), check_bound(x[j1], G::inv_bound(s + 1));
                 }
             },
             [&](auto qc) CF_INL {
@@ -529,7 +559,7 @@ struct PrimeRun {
             [&](auto jc) CF_INL { pin(x[decltype(jc)::value]); });
     }
     // Cyclic convolution of the registers (layout of pass 0, values < 4p) with the kernel 1/t;
-    // the result comes back in the same layout, in [0, 8p).
+    // the result comes back in the same layout, below INV_OUT p (below 2p for W).
     CF_HD void convolve() {
         if constexpr (NP == 1) {
             ex.each([&](int t, Regs<G>& rg) CF_INL {
@@ -905,9 +935,11 @@ struct PrimeRun {
                                 rg.x[j] = mont_mul(y, wrap ? fwrap : f[j % NCH], m);
                             } else {
                                 // p e[p]: with p floor(2^64/p) for the companion the quotient estimate
-                                // loses at most p (x < 8P) / 2^64 < 8 more, so pe < 12P
+                                // loses at most p x / 2^64 < INV_OUT more (x < INV_OUT P, p <= 2^14,
+                                // P < 2^50), so pe < (INV_OUT + 4) P
                                 const u64 pe = shoup_mul_lazy(rg.x[j], (u64)p, (u64)p * mu, P);
-                                const u64 y = shoup_mul_lazy(dv + 12 * P - pe, c, cq, P);
+                                check_bound(pe, G::INV_OUT + 4);
+                                const u64 y = shoup_mul_lazy(dv + (G::INV_OUT + 4) * P - pe, c, cq, P);
                                 rg.x[j] = mont_mul(y, wrap ? fwrap : f[j % NCH], m);
                             }
                             st_stream(col + p, rg.x[j]);

@@ -7,6 +7,8 @@
 #include <stdexcept>
 #include <vector>
 
+// every value bound the transforms rely on is checked here (suffix_engine.cuh: check_bound)
+#define CF_CHECK_BOUNDS 1
 #include "../../cuckoo-failure_b200/csrc/host_common.hpp"
 #include "../../cuckoo-failure_b200/csrc/suffix_engine.cuh"
 
@@ -138,6 +140,7 @@ static int emu_run(const uint64_t* primes, int B, int nmax, int d, int model, co
     }
     bool wide = false;  // the kernels for primes below 2^62, as the engine selects them
     for (int b = 0; b < B; ++b) wide = wide || primes[b] >= (1ull << 50);
+    try {
     switch (lg) {
         case 4: wide ? run_lg<4, true>(kp) : run_lg<4, false>(kp); break;
         case 5: wide ? run_lg<5, true>(kp) : run_lg<5, false>(kp); break;
@@ -151,6 +154,9 @@ static int emu_run(const uint64_t* primes, int B, int nmax, int d, int model, co
         case 13: wide ? run_lg<13, true>(kp) : run_lg<13, false>(kp); break;
         case 14: wide ? run_lg<14, true>(kp) : run_lg<14, false>(kp); break;
         default: return -4;
+    }
+    } catch (const std::runtime_error&) {
+        return -6;  // a value bound of the transforms did not hold (check_bound)
     }
     return err ? -5 : 0;
 }
