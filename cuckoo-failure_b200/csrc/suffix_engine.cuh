@@ -620,10 +620,12 @@ struct PrimeRun {
     // Stage-2 powers of h = 1/g(v) (row load) and h = g(v) (products), Montgomery form.  Rather
     // than an exponentiation per thread, the CTA builds at the start of each step a two-level
     // table per base in shared memory: A[k] = h^k (k < TA = min(T, 32)) at slots 0.., B[k] =
-    // h^(TA k) (k < TB = T / TA) at slots 32.., and h^T, h^(NCH T), h^L at slots 64, 65, 66.
-    // Thread t then starts its chains from A[t % TA] B[t / TA].  The 2 (TA + TB + 3) entries are
-    // independent exponentiations; task k runs on lane k / NW of warp k % NW, so every warp takes
-    // a few and none lags at the next barrier.
+    // h^(TA k) (k < TB = T / TA) at slots 32.., h^T and h^L at slots 64 and 66, and the chains'
+    // step h^(NCH T) as a plain residue with its Shoup companion at slots 65 and 67 (a Shoup
+    // product by it keeps a Montgomery-form power in Montgomery form).  Thread t starts its
+    // chains from A[t % TA] B[t / TA].  The 2 (TA + TB + 3) entries are independent
+    // exponentiations; task k runs on lane k / NW of warp k % NW, so every warp takes a few and
+    // none lags at the next barrier.
     static constexpr int TA = T < 32 ? T : 32, TB = T / TA;
     static constexpr int PW_TASKS = 2 * (TA + TB + 3);
     CF_HD void power_tables(int v) {
@@ -640,17 +642,29 @@ struct PrimeRun {
                 else if (r == TA + TB) e = (u64)T, slot = 64;
                 else if (r == TA + TB + 1) e = (u64)NCH * T, slot = 65;
                 else e = (u64)L, slot = 66;
-                pw[base * Smem<G>::PW_STRIDE + slot] = mont_pow(h, e, m);
+                u64 y = mont_pow(h, e, m);
+                if (slot == 65) {
+                    y = from_mont(y, m);
+                    pw[base * Smem<G>::PW_STRIDE + 67] = shoup_companion(y, P);
+                }
+                pw[base * Smem<G>::PW_STRIDE + slot] = y;
             }
         });
     }
-    // chain c of thread t holds h^(t + jT) for j = c (mod NCH) and steps by h^(NCH T)
-    CF_HD void power_chains(int base, int t, const Mod& m, u64 (&f)[NCH], u64& step) const {
+    // chain c of thread t holds h^(t + jT) for j = c (mod NCH) in Montgomery form and steps by a
+    // Shoup product with (step, stepq) = h^(NCH T) and its companion: values in [0, 4p) for primes
+    // below 2^50; canonical for W, where mont_mul's full product is exact only below 2^62
+    CF_HD u64 chain_step(u64 f, u64 step, u64 stepq) const {
+        const u64 y = shoup_mul_lazy(f, step, stepq, P);
+        if constexpr (W) return canon(y);
+        return y;
+    }
+    CF_HD void power_chains(int base, int t, const Mod& m, u64 (&f)[NCH], u64& step, u64& stepq) const {
         const u64* pw = sm + Smem<G>::PW + base * Smem<G>::PW_STRIDE;
         f[0] = TB > 1 ? mont_mul(pw[t % TA], pw[32 + t / TA], m) : pw[t];
         const u64 hT = pw[64];
         for (int c = 1; c < NCH; ++c) f[c] = mont_mul(f[c - 1], hT, m);
-        step = pw[65];
+        step = pw[65], stepq = pw[67];
     }
 
     // g(v) and 1/g(v) in Montgomery form (g != 0 for v >= d0)
@@ -881,7 +895,10 @@ struct PrimeRun {
                         constexpr int j = decltype(jc)::value;
                         const int i = G::idx(0, t, j);
                         pin(rg.x[j]);
-                        rg.x[j] = canon(shoup_mul_lazy(shoup_mul_lazy(rg.x[j], c, cq, P), iv, ivq, P));
+                        // S is read only by the stage-2 Montgomery product, which takes factors
+                        // below 4p: for primes below 2^50 it is stored lazily reduced
+                        rg.x[j] = shoup_mul_lazy(shoup_mul_lazy(rg.x[j], c, cq, P), iv, ivq, P);
+                        if constexpr (W) rg.x[j] = canon(rg.x[j]);
                         if (i >= v && i < n) st_stream(col + i, rg.x[j]);
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
@@ -891,24 +908,24 @@ struct PrimeRun {
             ex.sync();  // column v of S is read below
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const Mod m = md();
-                u64 f[NCH], step;  // g^-(t + jT)
-                power_chains(0, t, m, f, step);
+                u64 f[NCH], step, stepq;  // g^-(t + jT)
+                power_chains(0, t, m, f, step, stepq);
                 // columns q <= d0 of S are zero (stage 1 skipped: row q of V is zero), never written
                 load_row(t, rg.x, S(), SS(), v, d0 + 1, v + 1);
                 window<E, WK>(
                     [&](auto jc) CF_INL {
                         constexpr int j = decltype(jc)::value;
                         pin(rg.x[j]);
-                        rg.x[j] = mont_mul(rg.x[j], f[j % NCH], m);
-                        f[j % NCH] = mont_mul(f[j % NCH], step, m);
+                        rg.x[j] = mont_mul(rg.x[j], f[j % NCH], m);  // x, f < 4p: exact, canonical
+                        f[j % NCH] = chain_step(f[j % NCH], step, stepq);
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
             convolve();
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const Mod m = md();
-                u64 f[NCH], step;  // g^(t + jT)
-                power_chains(1, t, m, f, step);
+                u64 f[NCH], step, stepq;  // g^(t + jT)
+                power_chains(1, t, m, f, step, stepq);
                 const u64 dv = val(D(), v);
                 u64* col = VS() + (size_t)(v - tile_v0(v)) * (n + 1);  // V[.][v], by row
                 const u64* Dt = D();
@@ -944,7 +961,7 @@ struct PrimeRun {
                             }
                             st_stream(col + p, rg.x[j]);
                         }
-                        f[j % NCH] = mont_mul(f[j % NCH], step, m);
+                        f[j % NCH] = chain_step(f[j % NCH], step, stepq);
                         if constexpr (W) pm = madd(pm, pmT, P);
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });

@@ -66,3 +66,17 @@ def test_emulated_kernel_62bit_primes():
         ps = cb.prime_range(5, 2, bits=62)
         for nmax, dd, qq in ((64, 2, [(64, 200), (10, 11)]), (1000, 3, [(1000, 1500)])):
             assert h.emu_residues(ps, nmax, dd, qq, model) == [h.oracle_residues(p, nmax, dd, qq, model) for p in ps]
+
+
+@pytest.mark.parametrize("name", ["fast62_n4096_d2.txt", "fast_n4096_d3.txt"])
+def test_emulated_kernel_golden_n4096(name):
+    """L = 4096 against the reference's residues, 62-bit and 50-bit primes: chain values and
+    transform sums near their bounds occur only at this size and with primes near the top of the
+    list (a lazy chain value above 2^62 once broke the 62-bit kernel's Montgomery products)."""
+    d, queries, first, count, lines = h.load_fast_golden(name)
+    exp = h.expected_by_prime(lines)
+    items = sorted(exp.items())[:2]
+    qs = [q for q in queries if all(q in want for _, want in items)]
+    got = h.emu_residues([p for (i, p), _ in items], max(n for n, _ in qs), d, qs)
+    for ((i, p), want), row in zip(items, got):
+        assert row == [want[q] for q in qs], (name, i)
