@@ -3,6 +3,8 @@
 
 One step = one batch of B primes through the hot path: per-prime tables, the n-1 suffix-table
 steps (two 1/t convolutions each), the nbad(n, M) query and the Horner finish, for every prime.
+The device-timed step replays the batch captured once as a CUDA graph (cf_batch_graph_*); the
+e2e figure goes through cf_residues with host buffers.
 A prime-residue is one (d, prime) table built to n plus the residue of its query.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
@@ -32,7 +34,7 @@ K_OPS_PER_MM = 20  # INT32 multiply ops per 64-bit modular multiplication (fixed
 # DRAM bytes (read + write) per launch of the engine kernel, from the ncu launch list of this
 # bench's own command (profiles/k_suffix_n16384_b148_launches.md), keyed by (n, M, d, primes per
 # launch, prime bits)
-MEASURED_TRAFFIC = {(16384, 32768, 3, 148, 50): 1390.6e9 + 944.9e9}
+MEASURED_TRAFFIC = {(16384, 32768, 3, 148, 50): 1341.6e9 + 993.8e9}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 
@@ -86,6 +88,16 @@ class ClockSampler:
         reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows)}
+
+
+def hbm_peak():
+    """Copy bandwidth of this pool's B200s (GB/s): the measured-peaks file beside this script, else
+    the earlier measurement on the same pool."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
 
 
 def host_cores():
@@ -197,6 +209,7 @@ def main():
                     help="prime list: below 2^50 (default) or below 2^62 (the reference's -DFP_RB=64 build)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-query latency run")
+    ap.add_argument("--no-plain-form", action="store_true", help="skip the one-prime-per-launch timing")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the main kernel from an ncu capture (roofline.traffic)")
@@ -262,11 +275,15 @@ def main():
     d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
     d_out = torch.empty(B * J, dtype=torch.int64, device="cuda")
 
+    # the batch as one CUDA graph (error-word reset + the persistent launch), replayed every step
+    graph = eng.batch_graph(d_primes.data_ptr(), B, n, d, queries, d_out.data_ptr())
+
     def step():
-        eng.residues_async(d_primes.data_ptr(), B, n, d, queries, d_out.data_ptr(), stream.cuda_stream)
+        graph.launch(stream.cuda_stream)
 
     for _ in range(a.warmup):
         step()
+    graph.status(stream.cuda_stream)
     torch.cuda.synchronize()
     # self-check against the reference's residues for the primes it covers
     got = d_out.cpu().numpy().view(np.uint64)
@@ -291,11 +308,13 @@ def main():
         e0.record(stream)
         for _ in range(a.steps):
             step()
-            launches += eng.last_launches()
+            launches += graph.launches()
         e1.record(stream)
         barrier()
+    graph.status(stream.cuda_stream)
     ms = max_over_ranks(e0.elapsed_time(e1))
     value = world * B * a.steps / (ms * 1e-3)
+    graph.close()  # its workspace (about 1 GiB per prime) goes back before the e2e run allocates the engine's
 
     # end to end through the public API with host buffers (copies inside the timed region)
     host_primes = np.array(primes, dtype=np.uint64)
@@ -309,12 +328,30 @@ def main():
            "d2h_bytes_per_step": 8 * B * J + 4}
     assert np.array_equal(res.reshape(-1), got[:B * J]), "e2e residues differ from the device-timed run"
 
+    # the plain form: one launch per prime (B = 1), the same n, M, d, one launch on the same stream
+    plain = None
+    if not a.no_plain_form:
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        eng.residues_async(d_primes.data_ptr(), 1, n, d, queries, d_out.data_ptr(), stream.cuda_stream)
+        q1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = max_over_ranks(q0.elapsed_time(q1))
+        plain = {"value": world / (plain_ms * 1e-3), "unit": UNIT, "ms_per_prime": plain_ms,
+                 "what": "one launch per prime (batch of 1), same n, M, d and kernel, timed alone"}
+
     probe = ctypes.CDLL(os.path.join(PKG, "lib", "libcuckoo_b200_probe.so"))
     probe.cfp_imad_ops_per_s.restype = ctypes.c_double
     probe.cfp_imad_ops_per_s.argtypes = [ctypes.c_int, ctypes.c_int]
     peak = probe.cfp_imad_ops_per_s(local, 5) / 1e12
     # the timed stream holds only this engine's launches, back to back: per-GPU algorithmic rate
     achieved = B * a.steps * algorithmic_mm(n) * K_OPS_PER_MM / (ms * 1e-3) / 1e12
+    traffic = a.traffic_bytes or MEASURED_TRAFFIC.get((n, M, d, B, a.prime_bits))
+    hbm = None
+    if traffic:  # the kernel's DRAM bytes per launch (ncu) over its device-timed launch duration
+        gbs = traffic / (ms / a.steps * 1e-3) / 1e9
+        peak_gbs, which = hbm_peak()
+        hbm = {"achieved": gbs, "peak": peak_gbs, "unit": "GB/s", "frac": gbs / peak_gbs, "peak_source": which}
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(reference_binary()[0]):
         cpu = cpu_baseline(n, M, d)
@@ -331,11 +368,11 @@ def main():
                        "l2": "inputs larger than L2 (per-prime tables total far above 126 MB)"},
             "roofline": {"bound": "int32", "achieved": achieved, "peak": peak, "unit": "Top/s (INT32 IMAD)",
                          "frac": achieved / peak if peak else None,
-                         "traffic": a.traffic_bytes or MEASURED_TRAFFIC.get((n, M, d, B, a.prime_bits)),
+                         "traffic": traffic, "hbm": hbm,
                          "model": f"{K_OPS_PER_MM} INT32 multiply ops per modular multiplication, "
                                   f"{algorithmic_mm(n):.3e} multiplications per prime-residue; peak measured live"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-            "serving": serving}))
+            "plain_form": plain, "serving": serving}))
     if dist:
         dist.destroy_process_group()
     return 0

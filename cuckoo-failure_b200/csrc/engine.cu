@@ -182,8 +182,9 @@ static long fit_batch(size_t per_prime) {
     return (long)((fr - reserve) / per_prime);
 }
 
+// fixed_ws: use the workspace as it is (a graph capture, where nothing may be allocated)
 static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int d, int model, int J, const Plan& pl,
-                        u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0) {
+                        u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0, bool fixed_ws = false) {
     const KInfo ki = kernel_for(pl.lg, pl.wide);
     if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ki.smem),
@@ -191,7 +192,8 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
     const size_t per_prime = pl.ws_words * 8;
     // chunk: as many primes as the workspace (grown once) holds
     long cap = (long)(e->ws_bytes / per_prime);
-    if (cap < B) {
+    if (fixed_ws && cap < 1) return fail(e, CF_ERR_NOMEM, "workspace holds no prime");
+    if (cap < B && !fixed_ws) {
         long fitb = fit_batch(per_prime) + cap;  // what is free plus what is already held
         if (fitb < 1) return fail(e, CF_ERR_NOMEM, "not enough device memory for one prime");
         const long want = std::min<long>(B, fitb);
@@ -484,5 +486,105 @@ int cf_residues(cf_engine* e, const uint64_t* primes, int B, int nmax, int d, in
     if (herr) return fail(e, CF_ERR_DEVICE, "device check failed (code " + std::to_string(herr) + ")");
     return CF_OK;
 }
+
+struct cf_batch_graph {
+    int device = 0;
+    u64* ws = nullptr;  // the batch's own workspace, query table and error word
+    size_t ws_bytes = 0;
+    int* d_q = nullptr;
+    int qcap = 0;
+    int* d_err = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long launches = 0;
+};
+
+void cf_batch_graph_destroy(cf_batch_graph* g) {
+    if (!g) return;
+    cudaSetDevice(g->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    cudaFree(g->ws);
+    cudaFree(g->d_q);
+    cudaFree(g->d_err);
+    delete g;
+}
+
+int cf_batch_graph_create(cf_engine* e, const uint64_t* d_primes, int B, int nmax, int d, int model, const int* qn,
+                          const int* qM, int J, uint64_t* d_residues, cf_batch_graph** out) {
+    if (!e || !out) return CF_ERR_ARG;
+    *out = nullptr;
+    e->err.clear();
+    e->launches = 0;
+    if (B < 1 || !d_primes || (J > 0 && !d_residues)) return fail(e, CF_ERR_ARG, "bad batch buffers");
+    Plan pl;
+    int rc = plan(e, nmax, d, model, qn, qM, J, pl);
+    if (rc) return rc;
+    pl.wide = e->prime_bits > 50;
+    CF_CUDA(cudaSetDevice(e->device), "set device");
+    cf_batch_graph* g = new cf_batch_graph();
+    g->device = e->device;
+    cudaStream_t cs = nullptr;
+    // The graph's buffers stand in for the engine's while the batch is sized and captured, so the
+    // captured launches address them; the engine's own come back afterwards.
+    std::swap(e->ws, g->ws), std::swap(e->ws_bytes, g->ws_bytes), std::swap(e->d_q, g->d_q), std::swap(e->qcap, g->qcap),
+        std::swap(e->d_err, g->d_err);
+    auto run = [&]() -> int {
+        CF_CUDA(cudaMalloc(&e->d_err, sizeof(int)), "error word");
+        CF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
+        int r = ensure_queries(e, qn, qM, J, cs);
+        if (r) return r;
+        // allocate the workspace outside the capture: the captured call then finds it in place
+        const size_t per_prime = pl.ws_words * 8;
+        const long fitb = fit_batch(per_prime);
+        if (fitb < 1) return fail(e, CF_ERR_NOMEM, "not enough device memory for one prime");
+        r = ensure_ws(e, (size_t)std::min<long>(B, fitb) * per_prime);
+        if (r) return r;
+        const KInfo ki = kernel_for(pl.lg, pl.wide);
+        if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
+        CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ki.smem),
+                "shared memory attribute");
+        CF_CUDA(cudaStreamSynchronize(cs), "query upload");
+        CF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+        r = launch_batch(e, d_primes, B, nmax, d, model, J, pl, d_residues, cs, nullptr, 0, true);
+        cudaGraph_t gr = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(cs, &gr);
+        g->graph = gr;
+        if (r) return r;
+        CF_CUDA(ce, "end capture");
+        CF_CUDA(cudaGraphInstantiate(&g->exec, g->graph, 0), "graph instantiation");
+        g->launches = e->launches;
+        return CF_OK;
+    };
+    rc = run();
+    std::swap(e->ws, g->ws), std::swap(e->ws_bytes, g->ws_bytes), std::swap(e->d_q, g->d_q), std::swap(e->qcap, g->qcap),
+        std::swap(e->d_err, g->d_err);
+    if (cs) cudaStreamDestroy(cs);
+    if (rc) {
+        cf_batch_graph_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return CF_OK;
+}
+
+int cf_batch_graph_launch(cf_batch_graph* g, void* stream) {
+    if (!g || !g->exec) return CF_ERR_ARG;
+    if (cudaSetDevice(g->device) != cudaSuccess) return CF_ERR_CUDA;
+    return cudaGraphLaunch(g->exec, (cudaStream_t)stream) == cudaSuccess ? CF_OK : CF_ERR_CUDA;
+}
+
+int cf_batch_graph_status(cf_batch_graph* g, void* stream) {
+    if (!g) return CF_ERR_ARG;
+    if (cudaSetDevice(g->device) != cudaSuccess) return CF_ERR_CUDA;
+    int herr = 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(&herr, g->d_err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return CF_ERR_CUDA;
+    return herr ? CF_ERR_DEVICE : CF_OK;
+}
+
+long cf_batch_graph_launches(const cf_batch_graph* g) { return g ? g->launches : 0; }
 
 }  // extern "C"

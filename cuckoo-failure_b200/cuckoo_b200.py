@@ -84,6 +84,18 @@ def lib():
         L.cf_engine_set_prime_bits.restype = ctypes.c_int
         L.cf_last_launches.argtypes = [ctypes.c_void_p]
         L.cf_last_launches.restype = ctypes.c_long
+        L.cf_batch_graph_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, _intp, _intp, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.POINTER(ctypes.c_void_p)]
+        L.cf_batch_graph_create.restype = ctypes.c_int
+        L.cf_batch_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.cf_batch_graph_launch.restype = ctypes.c_int
+        L.cf_batch_graph_status.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.cf_batch_graph_status.restype = ctypes.c_int
+        L.cf_batch_graph_launches.argtypes = [ctypes.c_void_p]
+        L.cf_batch_graph_launches.restype = ctypes.c_long
+        L.cf_batch_graph_destroy.argtypes = [ctypes.c_void_p]
+        L.cf_batch_graph_destroy.restype = None
         _lib = L
     return _lib
 
@@ -173,6 +185,10 @@ class Engine:
                                      ctypes.c_void_p(d_out_ptr), ctypes.c_void_p(stream_ptr or 0))
         self._check(rc)
 
+    def batch_graph(self, d_primes_ptr, B, nmax, d, queries, d_out_ptr, model=MODEL_SUBSET):
+        """Capture one batch over device buffers as a CUDA graph (cf_batch_graph_create) for replay."""
+        return BatchGraph(self, d_primes_ptr, B, nmax, d, queries, d_out_ptr, model)
+
     def tables(self, primes, nmax, Fmax, d, model=MODEL_SUBSET):
         """Build and keep the suffix tables of `primes` on the device for later queries."""
         return Tables(self, primes, nmax, Fmax, d, model)
@@ -182,6 +198,52 @@ class Engine:
 
     def last_launches(self):
         return int(lib().cf_last_launches(self._h))
+
+
+class BatchGraph:
+    """A batch captured once as a CUDA graph with its own workspace; launch() replays it on a stream,
+    reading the primes from and writing the residues to the device buffers given at capture."""
+
+    def __init__(self, engine, d_primes_ptr, B, nmax, d, queries, d_out_ptr, model=MODEL_SUBSET):
+        qn, qM = _queries(queries)
+        h = ctypes.c_void_p()
+        rc = lib().cf_batch_graph_create(engine._h, ctypes.c_void_p(d_primes_ptr), B, nmax, d, model,
+                                         qn.ctypes.data_as(_intp), qM.ctypes.data_as(_intp), len(qn),
+                                         ctypes.c_void_p(d_out_ptr), ctypes.byref(h))
+        engine._check(rc)
+        self._g = h
+
+    def launch(self, stream_ptr=None):
+        rc = lib().cf_batch_graph_launch(self._g, ctypes.c_void_p(stream_ptr or 0))
+        if rc != CF_OK:
+            raise EngineError(rc, "graph launch failed")
+
+    def status(self, stream_ptr=None):
+        """Wait for stream_ptr and raise if the last replay's device checks failed."""
+        rc = lib().cf_batch_graph_status(self._g, ctypes.c_void_p(stream_ptr or 0))
+        if rc != CF_OK:
+            raise EngineError(rc, "graph replay failed its device checks")
+
+    def launches(self):
+        """Kernel launches in one replay."""
+        return int(lib().cf_batch_graph_launches(self._g))
+
+    def close(self):
+        if getattr(self, "_g", None):
+            lib().cf_batch_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class Tables:

@@ -93,6 +93,27 @@ long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J);
 /* Kernel launches issued by the last cf_residues / cf_residues_async call. */
 long cf_last_launches(const cf_engine* e);
 
+/* ---- graph-captured batches (no counterpart in the reference) ----
+ * The reference re-issues about 12 launches per step from the host (fast/cuckoo_fast.cu:841-855).
+ * Here a batch is already one persistent launch per chunk of primes; a batch graph captures that
+ * launch sequence (error-word reset and kernel launches) once as a CUDA graph, so a repeated
+ * batch is replayed with a single cudaGraphLaunch and no per-call host work.  The graph owns its
+ * own workspace, query table and error word, sized at capture for (B, nmax, d, model, queries):
+ * later engine calls do not disturb it.  d_primes[B] and d_residues[B*J] are device buffers bound
+ * at capture; their contents may change between launches (new primes, same sizes).  Launches of
+ * one graph must not overlap on the GPU: they share its workspace. */
+typedef struct cf_batch_graph cf_batch_graph;
+int cf_batch_graph_create(cf_engine* e, const uint64_t* d_primes, int B, int nmax, int d, int model, const int* qn,
+                          const int* qM, int J, uint64_t* d_residues, cf_batch_graph** out);
+/* Enqueue one replay on `stream` (a cudaStream_t; NULL is the CUDA default stream). */
+int cf_batch_graph_launch(cf_batch_graph* g, void* stream);
+/* Wait for the work on `stream` and report the device-side checks of the graph's last replay:
+ * CF_OK, or CF_ERR_DEVICE (e.g. a prime without a root of unity of order L). */
+int cf_batch_graph_status(cf_batch_graph* g, void* stream);
+/* Kernel launches (persistent-kernel nodes) in one replay. */
+long cf_batch_graph_launches(const cf_batch_graph* g);
+void cf_batch_graph_destroy(cf_batch_graph* g);
+
 /* ---- resident tables for serving (no counterpart in the reference) ----
  * The reference rebuilds the suffix table for every run.  A served workload keeps, per (d, prime),
  * the whole table V and the factorial tables on the device, and answers later queries with
