@@ -124,10 +124,27 @@ CF_HD u64 shoup_mul_lazy(u64 a, u64 w, u64 wq, u64 p) {
     asm("mul.wide.u32 %0, %1, %2;" : "=l"(t1) : "r"(a0), "r"(q1));
     asm("mul.wide.u32 %0, %1, %2;" : "=l"(t2) : "r"(a1), "r"(q0));
     asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(q) : "r"(a1), "r"(q1), "l"((t1 >> 32) + (t2 >> 32)));
+    // a w - q p modulo 2^64 with the subtraction folded into the multiplies:
+    //   a0 w0 - q0 p0 = a0 w0 + q0 (2^32 - p0) - q0 2^32                       (one mad.wide)
+    //   high word += a0 w1 + a1 w0 + q0 (-p1 - 1) + q1 (2^32 - p0)  (mod 2^32)  (four mad.lo)
+    // (p odd, so 2^32 - p0 is a 32-bit value); the same value as a w - q p, two instructions fewer.
+    const u32 w0 = lo32(w), w1 = hi32(w), qa = lo32(q), qb = hi32(q), np0 = 0u - lo32(p), np1m = ~hi32(p);
+    u64 x, y;
+    u32 rl, rh;
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(x) : "r"(a0), "r"(w0));
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(y) : "r"(qa), "r"(np0), "l"(x));
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(rl), "=r"(rh) : "l"(y));
+    asm("mad.lo.u32 %0, %1, %2, %0;" : "+r"(rh) : "r"(a0), "r"(w1));
+    asm("mad.lo.u32 %0, %1, %2, %0;" : "+r"(rh) : "r"(a1), "r"(w0));
+    asm("mad.lo.u32 %0, %1, %2, %0;" : "+r"(rh) : "r"(qa), "r"(np1m));
+    asm("mad.lo.u32 %0, %1, %2, %0;" : "+r"(rh) : "r"(qb), "r"(np0));
+    u64 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(rl), "r"(rh));
+    return r;  // below 4p < 2^64
 #else
     const u64 q = wmul(a1, q1) + (wmul(a0, q1) >> 32) + (wmul(a1, q0) >> 32);
-#endif
     return a * w - q * p;  // exact modulo 2^64, and the true value is below 4p < 2^64
+#endif
 }
 
 // a w mod p in [0, 2p) for any 64-bit a, given w < p and wq = floor(w 2^64 / p).
