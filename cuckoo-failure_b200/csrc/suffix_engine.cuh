@@ -830,13 +830,30 @@ struct PrimeRun {
     // Row r of V or S into the registers (layout 0): the slot of index i gets entry i of the row
     // for lo <= i < hi, zero elsewhere.  Columns of earlier groups come from the blocks, those of
     // r's own group from the staging tile.
+    //
+    // In layout 0 slot j holds index i = t + jT, so when T is a multiple of 16 the column group of
+    // slot j is W0 + j T/16 and the entry's place in its block is the same for every slot.  The
+    // block cell of (P, W) is then linear in W on either side of h (block_cell's three cases):
+    // W < h: W a_lo + b_lo; W >= h: W h + b_hi.  That replaces blk_off's per-entry case analysis.
     CF_HD void load_row(int t, u64 (&x)[E], const u64* pool, const u64* tile, int r, int lo, int hi) const {
         const int n = kp.n, v0 = tile_v0(r), h = block_h(n);
         const u64* tl = tile + r;
+        if constexpr (T % TILE == 0) {
+            const int P = grp(r), W0 = (t - 1) >> 4;  // -1 for t = 0, whose slot 0 is never in range
+            const int a_lo = P < h ? h : 1, b_lo = P < h ? P : (P - h) * h, b_hi = P - h - 1 - h * h;
+            const u64* base = pool + ((size_t)((r - 1) & 15) << 4) + ((t - 1) & 15);
 #pragma unroll
-        for (int j = 0; j < E; ++j) {
-            const int i = G::idx(0, t, j);
-            x[j] = (i >= lo && i < hi) ? ld_stream(i < v0 ? pool + blk_off(r, i, h) : tl + (size_t)(i - v0) * (n + 1)) : 0;
+            for (int j = 0; j < E; ++j) {
+                const int i = t + j * T, wg = W0 + j * (T / TILE);  // column group
+                const int cell = wg < h ? wg * a_lo + b_lo : wg * h + b_hi;
+                x[j] = (i >= lo && i < hi) ? ld_stream(i < v0 ? base + ((size_t)cell << 8) : tl + (size_t)(i - v0) * (n + 1)) : 0;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                const int i = G::idx(0, t, j);
+                x[j] = (i >= lo && i < hi) ? ld_stream(i < v0 ? pool + blk_off(r, i, h) : tl + (size_t)(i - v0) * (n + 1)) : 0;
+            }
         }
     }
 
