@@ -34,7 +34,7 @@ K_OPS_PER_MM = 20  # INT32 multiply ops per 64-bit modular multiplication (fixed
 # DRAM bytes (read + write) per launch of the engine kernel, from the ncu launch list of this
 # bench's own command (profiles/k_suffix_n16384_b148_launches.md), keyed by (n, M, d, primes per
 # launch, prime bits)
-MEASURED_TRAFFIC = {(16384, 32768, 3, 148, 50): 1341.6e9 + 993.8e9}
+MEASURED_TRAFFIC = {(16384, 32768, 3, 148, 50): 1299.2e9 + 865.1e9}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 
