@@ -41,6 +41,17 @@ cfb::KInfo cf_kinfo_lg11();
 cfb::KInfo cf_kinfo_lg12();
 cfb::KInfo cf_kinfo_lg13();
 cfb::KInfo cf_kinfo_lg14();
+cfb::KInfo cf_kinfo_lg4_w();
+cfb::KInfo cf_kinfo_lg5_w();
+cfb::KInfo cf_kinfo_lg6_w();
+cfb::KInfo cf_kinfo_lg7_w();
+cfb::KInfo cf_kinfo_lg8_w();
+cfb::KInfo cf_kinfo_lg9_w();
+cfb::KInfo cf_kinfo_lg10_w();
+cfb::KInfo cf_kinfo_lg11_w();
+cfb::KInfo cf_kinfo_lg12_w();
+cfb::KInfo cf_kinfo_lg13_w();
+cfb::KInfo cf_kinfo_lg14_w();
 
 namespace {
 
@@ -56,7 +67,22 @@ std::mutex g_mu;
 u64* g_scratch_ptr[MAX_DEVICES] = {};
 std::string g_err;
 
-KInfo kernel_for(int lg) {
+// wide: some prime is 2^50 or above (the kernels for primes below 2^62)
+KInfo kernel_for(int lg, bool wide) {
+    if (wide) switch (lg) {
+            case 4: return cf_kinfo_lg4_w();
+            case 5: return cf_kinfo_lg5_w();
+            case 6: return cf_kinfo_lg6_w();
+            case 7: return cf_kinfo_lg7_w();
+            case 8: return cf_kinfo_lg8_w();
+            case 9: return cf_kinfo_lg9_w();
+            case 10: return cf_kinfo_lg10_w();
+            case 11: return cf_kinfo_lg11_w();
+            case 12: return cf_kinfo_lg12_w();
+            case 13: return cf_kinfo_lg13_w();
+            case 14: return cf_kinfo_lg14_w();
+            default: return KInfo{nullptr, 0, 0, 0};
+        }
     switch (lg) {
         case 4: return cf_kinfo_lg4();
         case 5: return cf_kinfo_lg5();
@@ -114,23 +140,31 @@ extern "C" int cf_residues_noalloc(const uint64_t* primes, int B, int nmax, int 
     const u64 L = cfh::transform_length((u64)nmax);
     int lg = 0;
     while ((1ull << lg) < L) ++lg;
-    const KInfo ki = kernel_for(lg);
-    if (!ki.fn) return fail(CF_ERR_UNSUPPORTED, "transform length above 2^14 is not supported");
+    if (lg > 14) return fail(CF_ERR_UNSUPPORTED, "transform length above 2^14 is not supported");
+    bool wide = false;
     for (int b = 0; b < B; ++b) {
         const u64 p = primes[b];
-        if (p < 3 || (p & 1) == 0 || p >= (1ull << 50) || p <= (u64)F || (p - 1) % L != 0 || !cfh::is_prime(p))
-            return fail(CF_ERR_ARG, "prime " + std::to_string(p) + " is not an odd prime < 2^50 above max(n, M) with L | p-1");
+        if (p < 3 || (p & 1) == 0 || p >= (1ull << 62) || p <= (u64)F || (p - 1) % L != 0 || !cfh::is_prime(p))
+            return fail(CF_ERR_ARG, "prime " + std::to_string(p) + " is not an odd prime < 2^62 above max(n, M) with L | p-1");
+        if (p >= (1ull << 50)) wide = true;
     }
+    const KInfo ki = kernel_for(lg, wide);
+    if (!ki.fn) return fail(CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     if (B == 0) return CF_OK;
     const Layout lay = make_layout(nmax, F, (int)L, J, ki.threads >= 32 ? ki.threads / 32 : 1, ki.r);
-    // scratch layout: [error word][queries: J n's then J M's as ints][primes][residues][workspaces]
-    const size_t qwords = ((size_t)J + 1 + 31) & ~(size_t)31;
+    // scratch layout: [error word][queries: J n's then J M's as ints][primes][residues][workspaces],
+    // every region padded to 256 bytes
+    auto pad = [](size_t w) { return (w + 31) & ~(size_t)31; };
+    const size_t qwords = pad((size_t)J);  // J sizes n and J sizes M, 4 bytes each
     const size_t fixed = HEAD_WORDS + qwords;
-    const size_t per_prime = lay.total + 1 + (size_t)J;
-    if (fixed + per_prime + 32 > SCRATCH_WORDS)
-        return fail(CF_ERR_NOMEM, "a table of nmax = " + std::to_string(nmax) + " needs " + std::to_string(8 * (fixed + per_prime)) +
+    auto words_for = [&](size_t c) { return fixed + pad(c) + pad(c * (size_t)J) + c * lay.total; };
+    if (words_for(1) > SCRATCH_WORDS)
+        return fail(CF_ERR_NOMEM, "a table of nmax = " + std::to_string(nmax) + " needs " + std::to_string(8 * words_for(1)) +
                                       " bytes of scratch; the static scratch holds " + std::to_string(CF_NOALLOC_SCRATCH_BYTES) + " bytes");
-    const size_t cap = std::min<size_t>((SCRATCH_WORDS - fixed - 32) / per_prime, (size_t)B);
+    // primes per launch: as many as the padded layout holds
+    size_t cap = std::min<size_t>((SCRATCH_WORDS - fixed) / (lay.total + 1 + (size_t)J), (size_t)B);
+    cap = std::max<size_t>(cap, 1);
+    while (cap > 1 && words_for(cap) > SCRATCH_WORDS) --cap;
 
     u64* scr = nullptr;
     int rc = scratch_for_current_device(&scr);
@@ -140,9 +174,8 @@ extern "C" int cf_residues_noalloc(const uint64_t* primes, int B, int nmax, int 
     int* d_qn = (int*)(scr + HEAD_WORDS);
     int* d_qM = d_qn + J;
     u64* d_primes = scr + fixed;
-    u64* d_out = d_primes + ((cap + 31) & ~(size_t)31);
-    u64* d_ws = d_out + ((cap * (size_t)J + 31) & ~(size_t)31);
-    if (d_ws + cap * lay.total > scr + SCRATCH_WORDS) return fail(CF_ERR_NOMEM, "scratch layout overflow");
+    u64* d_out = d_primes + pad(cap);
+    u64* d_ws = d_out + pad(cap * (size_t)J);
 #define NA_CUDA(call, what)                                                                     \
     do {                                                                                        \
         cudaError_t c_ = (call);                                                                \

@@ -24,6 +24,7 @@ MODEL_SUBSET = 0
 MODEL_REPLACEMENT = 1
 
 CF_OK, CF_ERR_ARG, CF_ERR_CUDA, CF_ERR_NOMEM, CF_ERR_UNSUPPORTED, CF_ERR_DEVICE = 0, -1, -2, -3, -4, -5
+CF_NOALLOC_SCRATCH_BYTES = 64 << 20  # include/cuckoo_b200.h
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _intp = ctypes.POINTER(ctypes.c_int)

@@ -2,7 +2,10 @@
 """Multi-GPU runs of the batch engine: one process per GPU, each on its own contiguous slice of
 the prime range, with no exchange on the data path.  Rank 0 gathers the output lines (host
 objects, a few bytes per residue) and writes them in prime order, exactly the lines one
-`cuckoo_fast_b200 D QUERIES FIRST COUNT` process would print.
+`cuckoo_fast_b200 D QUERIES FIRST COUNT` process would print.  With --out the job resumes as the
+reference's driver does (fast/cuckoo_fast.cu:697-726): rank 0 reads the file, a prime counts as
+done only when every query that needs it has its line there, and only the remaining primes are
+split across the ranks and appended.
 
 The reference splits a run the same way, by FIRST COUNT per process (fast/README.md:23-25);
 this is that split inside one torchrun job:
@@ -38,6 +41,49 @@ def segments(first, count, needs):
     return out
 
 
+def done_primes(path, needs, first, count):
+    """Primes i in [first, first + count) already complete in the output file at `path`: the file
+    holds as many lines for i as there are queries with i < need (fast/cuckoo_fast.cu:697-720).
+    A prime cut off inside its lines counts as not done (its lines are all written again)."""
+    if not path or not os.path.exists(path):
+        return set()
+    cnt = {}
+    with open(path) as f:
+        for ln in f:
+            t = ln.split()
+            if len(t) == 5 and t[0].lstrip("-").isdigit():
+                cnt[int(t[0])] = cnt.get(int(t[0]), 0) + 1
+    out = set()
+    for i in range(first, first + count):
+        want = sum(1 for k in needs if i < k)
+        if want > 0 and cnt.get(i, 0) == want:
+            out.add(i)
+    return out
+
+
+def todo_primes(first, count, needs, done):
+    """Prime indices still to compute, in order (fast/cuckoo_fast.cu:722-726)."""
+    top = min(first + count, max(needs) if needs else first)
+    return [i for i in range(first, top) if i not in done]
+
+
+def shard_list(todo, rank, world):
+    """Rank's contiguous slice of the todo list (sizes differ by at most one)."""
+    f, c = shard(0, len(todo), rank, world)
+    return todo[f:f + c]
+
+
+def runs(indices):
+    """Maximal runs of consecutive indices: [(first, count)]."""
+    out = []
+    for i in indices:
+        if out and out[-1][0] + out[-1][1] == i:
+            out[-1] = (out[-1][0], out[-1][1] + 1)
+        else:
+            out.append((i, 1))
+    return out
+
+
 def rank_lines(d, queries, first, count, residues_fn, model=cb.MODEL_SUBSET):
     """Output records (i, p, n, M, residue) for primes first .. first+count-1, in order, only for
     queries with i < need(n, M) (fast/cuckoo_fast.cu:891-898).  residues_fn(primes, nmax, d,
@@ -66,6 +112,30 @@ def gather_to_rank0(records, dist):
     merged = [r for part in parts for r in part]
     merged.sort(key=lambda r: r[0])
     return merged
+
+
+def run_job(d, queries, first, count, residues_fn, out_path=None, dist=None, model=cb.MODEL_SUBSET):
+    """One job over all ranks: rank 0 finds the primes still to do (resuming from out_path), every
+    rank computes its contiguous share of them, rank 0 gathers and appends the lines to out_path
+    (or returns them as text).  Returns the text written on rank 0, None elsewhere."""
+    needs = [cb.need(n, M, d, model) for n, M in queries]
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist else (0, 1)
+    todo = [None]
+    if rank == 0:
+        todo[0] = todo_primes(first, count, needs, done_primes(out_path, needs, first, count))
+    if dist:
+        dist.broadcast_object_list(todo, src=0)
+    recs = []
+    for f, c in runs(shard_list(todo[0], rank, world)):
+        recs += rank_lines(d, queries, f, c, residues_fn, model)
+    merged = gather_to_rank0(recs, dist)
+    if merged is None:
+        return None
+    text = format_lines(merged)
+    if out_path:
+        with open(out_path, "a") as fo:
+            fo.write(text)
+    return text
 
 
 def max_over_ranks(x, dist, device=None):
@@ -106,18 +176,11 @@ def main(argv=None):
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
         dd = dist
-    first, count = shard(a.first, a.count, rank, world)
     with cb.Engine(local) as eng:
-        recs = rank_lines(a.d, queries, first, count,
-                          lambda ps, nm, d, qs, m: eng.residues(ps, nm, d, qs, model=m), model)
-    merged = gather_to_rank0(recs, dd)
-    if merged is not None:
-        text = format_lines(merged)
-        if a.out:
-            with open(a.out, "a") as f:
-                f.write(text)
-        else:
-            sys.stdout.write(text)
+        text = run_job(a.d, queries, a.first, a.count, lambda ps, nm, d, qs, m: eng.residues(ps, nm, d, qs, model=m),
+                       a.out, dd, model)
+    if text is not None and not a.out:
+        sys.stdout.write(text)
     if dd is not None:
         dist.destroy_process_group()
     return 0

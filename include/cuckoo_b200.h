@@ -138,9 +138,10 @@ void cf_tables_free(cf_tables* t);
  * fits up to about nmax = 4000; smaller tables are batched several primes per launch. */
 #define CF_NOALLOC_SCRATCH_BYTES (64ull << 20)
 
-/* The computation of cf_residues, for callers that cannot allocate device memory (their device
- * memory belongs to another allocator, allocation is forbidden where they run, or their device
- * footprint must stay fixed after start-up).  No engine, no cudaMalloc/cudaFree: all scratch is
+/* The computation of cf_residues (primes of either list, below 2^50 or below 2^62), for callers
+ * that cannot allocate device memory (their device memory belongs to another allocator,
+ * allocation is forbidden where they run, or their device footprint must stay fixed after
+ * start-up).  No engine, no cudaMalloc/cudaFree: all scratch is
  * a file-scope device array of CF_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
  * until exit.  Host buffers; runs on `stream` (NULL = default stream) of the current device and
  * returns when the residues are in `residues`.  The first call on a device resolves the array's

@@ -7,8 +7,14 @@ oracle/Makefile.ref into oracle/_ref/: the 64-bit batch engine's host build
 62-bit primes, -DFP_RB=64) and the 32-bit library CLI (src/cuckoo_fail.cpp).  They pin the oracle and the CUDA engine to the reference.
 
 Run from the repository root, where the reference tree is available:
-    make -f oracle/Makefile.ref && python tests/golden/make_golden.py
+    make -f oracle/Makefile.ref && python tests/golden/make_golden.py [--groups base,large]
+
+Groups: `base` (small sizes, config 2, one or two primes at n = 16384, the library CLI at small n)
+and `large` (the replacement model at n = 4096 and 16384 through the library's --mod P, 18 queries
+at n <= 16384, and a seeded sample of the uneven-batch workload).
 """
+import argparse
+import concurrent.futures as cf
 import os
 import re
 import subprocess
@@ -26,8 +32,9 @@ def fast_bin():
     return ifma if has_ifma and os.path.exists(ifma) else os.path.join(REF, "cuckoo_fast_cpu")
 
 
-def run_fast(d, queries, first, count, out_name, batch=None, binary=None):
-    """fast/cuckoo_fast.cu CLI: cuckoo_fast D QUERIES FIRST COUNT [--batch B] -> 'i p n M residue' lines."""
+def fast_lines(d, queries, first, count, batch=None, binary=None):
+    """fast/cuckoo_fast.cu CLI: cuckoo_fast D QUERIES FIRST COUNT [--batch B] -> its stdout
+    ('i p n M residue' lines)."""
     with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
         for n, M in queries:
             f.write(f"{n} {M}\n")
@@ -37,6 +44,11 @@ def run_fast(d, queries, first, count, out_name, batch=None, binary=None):
         cmd += ["--batch", str(batch)]
     out = subprocess.run(cmd, check=True, capture_output=True, text=True).stdout
     os.unlink(qpath)
+    return out
+
+
+def run_fast(d, queries, first, count, out_name, batch=None, binary=None):
+    out = fast_lines(d, queries, first, count, batch, binary)
     with open(os.path.join(HERE, out_name), "w") as g:
         g.write(f"# d={d} queries={' '.join(f'{n},{M}' for n, M in queries)} first={first} count={count}\n")
         g.write(out)
@@ -47,7 +59,73 @@ def run_lib(args):
     return subprocess.run([os.path.join(REF, "cuckoo_fail")] + args, check=True, capture_output=True, text=True).stdout
 
 
+def lib_mod(n, M, d, P, rep):
+    """`cuckoo_fail single ... --mod P` -> the residue line of lib_cuckoo_fail.txt's 'mod' form."""
+    t = run_lib(["single", "-n", str(n), "-M", str(M), "-d", str(d), "--mod", str(P)] + (["--replacement"] if rep else []))
+    r = re.search(r"N_bad mod (\d+) = (\d+)", t)
+    return f"mod {int(rep)} {n} {M} {d} {r.group(1)} {r.group(2)}"
+
+
+def large():
+    """Full-size pins: the replacement model (no 50-bit reference exists, the fast engine hard-codes
+    C(v, d)) through the library at the primes it would choose itself; 18 queries at n <= 16384
+    against the host build; a seeded sample of the uneven-batch workload."""
+    sys.path.insert(0, os.path.join(ROOT, "cuckoo-failure_b200"))
+    import numpy as np
+
+    import cuckoo_b200 as cb
+    import uneven
+
+    jobs = {}
+    with cf.ThreadPoolExecutor(max(1, (os.cpu_count() or 2) - 1)) as ex:
+        # 1. library --mod P: the first two primes of the library's own list for each case
+        for n, M, d, rep in ((16384, 32768, 3, True), (4096, 8192, 3, True), (4096, 8192, 3, False)):
+            for P in cb.lib_primes(n, M, d, int(rep))[:2]:
+                jobs[("lib", n, M, d, P, rep)] = ex.submit(lib_mod, n, M, d, P, rep)
+        # 2. 18 queries with n in [1000, 16384] (16384 included), M in [1.5 n, 4 n], primes 0 and 1
+        rng = np.random.default_rng(18)
+        ns = [16384] + sorted({int(x) for x in np.exp(rng.uniform(np.log(1000), np.log(16384), 17))}, reverse=True)
+        qJ = [(n, int(round(n * rng.uniform(1.5, 4.0)))) for n in ns]
+        jobs[("J18",)] = ex.submit(fast_lines, 3, qJ, 0, 2)
+        # 3. the first 16 instances of the uneven-batch workload, grouped by d as one table set per d
+        #    serves them: primes 0 and 1 (every instance active), and each instance's last prime
+        #    need - 1 (only the instances that still need it active)
+        insts = uneven.instances(16)
+        byd = {}
+        for n, M, d in insts:
+            byd.setdefault(d, []).append((n, M))
+        for d, qs in byd.items():
+            jobs[("unev", d, 0)] = ex.submit(fast_lines, d, qs, 0, 2)
+            for n, M in qs:
+                k = cb.need(n, M, d) - 1
+                if ("unev", d, k) not in jobs:
+                    jobs[("unev", d, k)] = ex.submit(fast_lines, d, qs, k, 1)
+        res = {k: f.result() for k, f in jobs.items()}
+    with open(os.path.join(HERE, "lib_large.txt"), "w") as g:
+        g.write("# 'mod rep n M d P residue' from the library CLI (cuckoo_fail single ... --mod P), P among the "
+                "first primes of the library's own list for (n, M, d)\n")
+        g.write("".join(v + "\n" for k, v in sorted(res.items(), key=lambda kv: str(kv[0])) if k[0] == "lib"))
+    with open(os.path.join(HERE, "fast_n16384_d3_J18.txt"), "w") as g:
+        g.write(f"# d=3 queries={' '.join(f'{n},{M}' for n, M in qJ)} first=0 count=2\n")
+        g.write(res[("J18",)])
+    with open(os.path.join(HERE, "uneven_sample.txt"), "w") as g:
+        g.write(f"# uneven.instances(16) (seed {uneven.CONFIG4_SEED}): "
+                + " ".join(f"{n},{M},{d}" for n, M, d in insts) + "\n")
+        g.write("# 'd i p n M residue' from the host build, one run per d over that d's instances\n")
+        for k in sorted(k for k in res if k[0] == "unev"):
+            for ln in res[k].splitlines():
+                g.write(f"{k[1]} {ln}\n")
+    print("large fixtures written")
+
+
 def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--groups", default="base,large")
+    groups = ap.parse_args().groups.split(",")
+    if "large" in groups:
+        large()
+    if "base" not in groups:
+        return 0
     small = [(8, 9), (8, 20), (37, 50), (100, 150), (200, 400), (255, 256), (256, 600), (300, 301), (512, 1024)]
     for d in (2, 3, 4):
         run_fast(d, small, 0, 40, f"fast_small_d{d}.txt")

@@ -136,3 +136,23 @@ def expected_by_prime(lines):
     for i, p, n, M, r in lines:
         out.setdefault((i, p), {})[(n, M)] = r
     return out
+
+
+def load_lib_large():
+    """tests/golden/lib_large.txt: [(rep, n, M, d, P, residue)] from the library CLI's --mod P."""
+    out = []
+    with open(os.path.join(GOLDEN, "lib_large.txt")) as f:
+        for ln in f:
+            t = ln.split()
+            if t and t[0] == "mod":
+                out.append(tuple(int(x) for x in t[1:]))
+    return out
+
+
+def load_uneven_sample():
+    """tests/golden/uneven_sample.txt: (instances [(n, M, d)], records [(d, i, p, n, M, residue)])."""
+    with open(os.path.join(GOLDEN, "uneven_sample.txt")) as f:
+        head = f.readline()
+        insts = [tuple(int(x) for x in tok.split(",")) for tok in head.split(":", 1)[1].split()]
+        recs = [tuple(int(x) for x in ln.split()) for ln in f if ln.strip() and not ln.startswith("#")]
+    return insts, recs

@@ -42,6 +42,47 @@ def _rank_main(rank, world, port, d, queries, first, count, out_path):
         dist.destroy_process_group()
 
 
+def _resume_main(rank, world, port, d, queries, first, count, out_path):
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.join(h.ROOT, "cuckoo-failure_b200"))
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        multi.run_job(d, queries, first, count, oracle_residues_fn, out_path, dist)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_resume_from_a_file_cut_inside_a_prime(tmp_path):
+    """Primes 0..9 complete and prime 10 cut after one of its lines: the job recomputes primes
+    10..23 only and appends them, as the reference driver does (the cut lines stay)."""
+    d, queries, first, count, lines = h.load_fast_golden("fast_small_d3.txt")
+    queries = [q for q in queries if q[0] <= 300]
+    count = 24
+    full = [ln for ln in lines if ln[0] < count and (ln[2], ln[3]) in queries]
+    fmt = lambda lns: "".join(" ".join(map(str, ln)) + "\n" for ln in lns)
+    head = [ln for ln in full if ln[0] < 10] + [ln for ln in full if ln[0] == 10][:1]
+    out = tmp_path / "resumed.txt"
+    out.write_text(fmt(head))
+    mp.start_processes(_resume_main, args=(2, free_port(), d, queries, first, count, str(out)), nprocs=2,
+                       join=True, start_method="spawn")
+    assert out.read_text() == fmt(head) + fmt([ln for ln in full if ln[0] >= 10])
+    # On a complete file nothing is left to do.  (A prime once cut keeps one line too many, so
+    # like the reference driver, whose rule is an exact line count, a later run redoes it.)
+    done = tmp_path / "complete.txt"
+    done.write_text(fmt(full))
+    mp.start_processes(_resume_main, args=(2, free_port(), d, queries, first, count, str(done)), nprocs=2,
+                       join=True, start_method="spawn")
+    assert done.read_text() == fmt(full)
+
+
+def test_todo_and_runs():
+    needs = [5, 12]
+    assert multi.todo_primes(0, 20, needs, {1, 2, 7}) == [0, 3, 4, 5, 6, 8, 9, 10, 11]
+    assert multi.runs([0, 3, 4, 5, 6, 8, 9, 10, 11]) == [(0, 1), (3, 4), (8, 4)]
+    assert multi.shard_list(list(range(9)), 0, 2) + multi.shard_list(list(range(9)), 1, 2) == list(range(9))
+
+
 def test_shard_is_disjoint_and_covering():
     for count in (0, 1, 7, 40, 14184):
         for world in (1, 2, 3, 8):

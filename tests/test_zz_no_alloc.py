@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import cuckoo_b200 as cb
+import helpers as h
 
 pytestmark = pytest.mark.gpu
 
@@ -49,3 +50,38 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls():
 def test_noalloc_rejects_tables_beyond_the_scratch():
     rc, _, msg = noalloc(cb.prime_range(0, 1), 8000, 3, [(8000, 16000)])
     assert rc == cb.CF_ERR_NOMEM and "static scratch" in msg
+
+
+def test_noalloc_matches_reference_fixtures():
+    """Pinned directly to the reference's residues (50-bit and 62-bit lists), not only to cf_residues."""
+    for name in ("fast_small_d3.txt", "fast_n300_first17.txt", "fast62_small_d3.txt"):
+        d, queries, first, count, lines = h.load_fast_golden(name)
+        exp = h.expected_by_prime(lines)
+        primes = [p for (i, p) in sorted(exp)]
+        rc, got, msg = noalloc(primes, max(n for n, _ in queries), d, queries)
+        assert rc == cb.CF_OK, msg
+        for k, (ip, want) in enumerate(sorted(exp.items())):
+            assert {q: int(r) for q, r in zip(queries, got[k]) if q in want} == want, (name, ip)
+
+
+def largest_fitting_nmax():
+    """The largest nmax (one query (nmax, nmax + 1)) whose single-prime scratch layout fits:
+    a 256-byte error word, then queries, primes, residues and one workspace, each padded to 256 bytes."""
+    words = cb.CF_NOALLOC_SCRATCH_BYTES // 8
+    fits = lambda n: 4 * 32 + cb.workspace_bytes(n, n + 1, 1) // 8 <= words
+    lo, hi = 16, 16384
+    while lo < hi:
+        mid = (lo + hi + 1) // 2
+        lo, hi = (mid, hi) if fits(mid) else (lo, mid - 1)
+    return lo
+
+
+def test_noalloc_at_the_scratch_limit():
+    n = largest_fitting_nmax()
+    primes = cb.prime_range(0, 2)
+    rc, got, msg = noalloc(primes, n, 3, [(n, n + 1)])
+    assert rc == cb.CF_OK, msg  # fits exactly: two launches of one prime each
+    with cb.Engine(0) as eng:
+        assert np.array_equal(got, eng.residues(primes, n, 3, [(n, n + 1)]))
+    rc, _, msg = noalloc(primes[:1], n + 1, 3, [(n + 1, n + 2)])
+    assert rc == cb.CF_ERR_NOMEM and "static scratch" in msg, msg
