@@ -9,36 +9,15 @@
 #include <vector>
 
 #include "../../include/cuckoo_b200.h"
+#include "engine_internal.hpp"
 #include "host_common.hpp"
 #include "kernel_lg.cuh"
 #include "table_query.cuh"
 
 using namespace cfb;
 
-cfb::KInfo cf_kinfo_lg4();
-cfb::KInfo cf_kinfo_lg5();
-cfb::KInfo cf_kinfo_lg6();
-cfb::KInfo cf_kinfo_lg7();
-cfb::KInfo cf_kinfo_lg8();
-cfb::KInfo cf_kinfo_lg9();
-cfb::KInfo cf_kinfo_lg10();
-cfb::KInfo cf_kinfo_lg11();
-cfb::KInfo cf_kinfo_lg12();
-cfb::KInfo cf_kinfo_lg13();
-cfb::KInfo cf_kinfo_lg14();
-cfb::KInfo cf_kinfo_lg4_w();
-cfb::KInfo cf_kinfo_lg5_w();
-cfb::KInfo cf_kinfo_lg6_w();
-cfb::KInfo cf_kinfo_lg7_w();
-cfb::KInfo cf_kinfo_lg8_w();
-cfb::KInfo cf_kinfo_lg9_w();
-cfb::KInfo cf_kinfo_lg10_w();
-cfb::KInfo cf_kinfo_lg11_w();
-cfb::KInfo cf_kinfo_lg12_w();
-cfb::KInfo cf_kinfo_lg13_w();
-cfb::KInfo cf_kinfo_lg14_w();
 // The kernel for transform length 2^lg: primes below 2^50, or (wide) below 2^62.
-static KInfo kernel_for(int lg, bool wide = false) {
+KInfo kernel_for(int lg, bool wide) {
     if (wide) switch (lg) {
             case 4: return cf_kinfo_lg4_w();
             case 5: return cf_kinfo_lg5_w();
@@ -68,41 +47,6 @@ static KInfo kernel_for(int lg, bool wide = false) {
         default: return KInfo{nullptr, 0, 0, 0};
     }
 }
-static constexpr int MAX_LG = 14;
-
-// ------------------------------------------------------------------------------------------
-// Engine
-// ------------------------------------------------------------------------------------------
-struct cf_engine {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    u64* ws = nullptr;  // workspace
-    size_t ws_bytes = 0;
-    int* d_err = nullptr;
-    int* d_q = nullptr;  // [2][qcap] query n and M
-    int qcap = 0;
-    u64* d_primes = nullptr;  // staging for cf_residues
-    u64* d_out = nullptr;
-    size_t io_cap = 0;  // primes capacity of d_primes; d_out has io_cap * jcap
-    int jcap = 0;
-    long launches = 0;
-    int prime_bits = 50;  // for cf_residues_async, whose primes are not read on the host
-    std::string err;
-};
-
-static int fail(cf_engine* e, int code, const std::string& msg) {
-    if (e) e->err = msg;
-    return code;
-}
-static int cuda_fail(cf_engine* e, cudaError_t c, const char* what) {
-    return fail(e, CF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(c));
-}
-#define CF_CUDA(call, what)                              \
-    do {                                                 \
-        cudaError_t c_ = (call);                         \
-        if (c_ != cudaSuccess) return cuda_fail(e, c_, what); \
-    } while (0)
-
 struct Plan {
     int lg, F, d0;
     bool wide = false;  // some prime is 2^50 or above: the kernels for primes below 2^62
@@ -182,12 +126,27 @@ static long fit_batch(size_t per_prime) {
     return (long)((fr - reserve) / per_prime);
 }
 
+// A launch keeps the per-warp partial sums of its J queries in shared memory (8 J words per warp)
+// beside the kernel's fixed part; more queries than the block's opt-in limit allows are refused.
+int check_smem(cf_engine* e, size_t smem, int J) {
+    int dev = 0, optin = 0;
+    CF_CUDA(cudaGetDevice(&dev), "current device");
+    CF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "shared memory limit");
+    if (smem > (size_t)optin)
+        return fail(e, CF_ERR_UNSUPPORTED, std::to_string(J) + " queries need " + std::to_string(smem) +
+                                               " bytes of shared memory per block; the device allows " + std::to_string(optin));
+    return CF_OK;
+}
+
 // fixed_ws: use the workspace as it is (a graph capture, where nothing may be allocated)
 static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int d, int model, int J, const Plan& pl,
                         u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0, bool fixed_ws = false) {
     const KInfo ki = kernel_for(pl.lg, pl.wide);
     if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
-    CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ki.smem),
+    const size_t smem = ki.smem_for(J);
+    int rc0 = check_smem(e, smem, J);
+    if (rc0) return rc0;
+    CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
             "shared memory attribute");
     const size_t per_prime = pl.ws_words * 8;
     // chunk: as many primes as the workspace (grown once) holds
@@ -224,7 +183,7 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
         kp.err = e->d_err;
         kp.keep = keep ? keep + (size_t)at * keep_words : nullptr;
         kp.keep_words = keep_words;
-        ki.fn<<<nb, ki.threads, ki.smem, s>>>(kp);
+        ki.fn<<<nb, ki.threads, smem, s>>>(kp);
         CF_CUDA(cudaGetLastError(), "kernel launch");
         ++e->launches;
     }
@@ -542,8 +501,6 @@ int cf_batch_graph_create(cf_engine* e, const uint64_t* d_primes, int B, int nma
         if (r) return r;
         const KInfo ki = kernel_for(pl.lg, pl.wide);
         if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
-        CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ki.smem),
-                "shared memory attribute");
         CF_CUDA(cudaStreamSynchronize(cs), "query upload");
         CF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
         r = launch_batch(e, d_primes, B, nmax, d, model, J, pl, d_residues, cs, nullptr, 0, true);

@@ -1,0 +1,74 @@
+// Internals shared by the C ABI's translation units (engine.cu, uneven.cu): the engine object,
+// its error helpers and the kernel table.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/cuckoo_b200.h"
+#include "kernel_lg.cuh"
+
+using cfb::u64;
+
+cfb::KInfo cf_kinfo_lg4();
+cfb::KInfo cf_kinfo_lg5();
+cfb::KInfo cf_kinfo_lg6();
+cfb::KInfo cf_kinfo_lg7();
+cfb::KInfo cf_kinfo_lg8();
+cfb::KInfo cf_kinfo_lg9();
+cfb::KInfo cf_kinfo_lg10();
+cfb::KInfo cf_kinfo_lg11();
+cfb::KInfo cf_kinfo_lg12();
+cfb::KInfo cf_kinfo_lg13();
+cfb::KInfo cf_kinfo_lg14();
+cfb::KInfo cf_kinfo_lg4_w();
+cfb::KInfo cf_kinfo_lg5_w();
+cfb::KInfo cf_kinfo_lg6_w();
+cfb::KInfo cf_kinfo_lg7_w();
+cfb::KInfo cf_kinfo_lg8_w();
+cfb::KInfo cf_kinfo_lg9_w();
+cfb::KInfo cf_kinfo_lg10_w();
+cfb::KInfo cf_kinfo_lg11_w();
+cfb::KInfo cf_kinfo_lg12_w();
+cfb::KInfo cf_kinfo_lg13_w();
+cfb::KInfo cf_kinfo_lg14_w();
+// The kernel for transform length 2^lg: primes below 2^50, or (wide) below 2^62 (engine.cu).
+cfb::KInfo kernel_for(int lg, bool wide = false);
+constexpr int MAX_LG = 14;
+struct cf_engine;
+// CF_OK if a launch with J queries fits the device's shared memory per block (engine.cu)
+int check_smem(cf_engine* e, size_t smem, int J);
+
+// ------------------------------------------------------------------------------------------
+// Engine
+// ------------------------------------------------------------------------------------------
+struct cf_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    u64* ws = nullptr;  // workspace
+    size_t ws_bytes = 0;
+    int* d_err = nullptr;
+    int* d_q = nullptr;  // [2][qcap] query n and M
+    int qcap = 0;
+    u64* d_primes = nullptr;  // staging for cf_residues
+    u64* d_out = nullptr;
+    size_t io_cap = 0;  // primes capacity of d_primes; d_out has io_cap * jcap
+    int jcap = 0;
+    long launches = 0;
+    int prime_bits = 50;  // for cf_residues_async, whose primes are not read on the host
+    std::string err;
+};
+
+inline int fail(cf_engine* e, int code, const std::string& msg) {
+    if (e) e->err = msg;
+    return code;
+}
+inline int cuda_fail(cf_engine* e, cudaError_t c, const char* what) {
+    return fail(e, CF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(c));
+}
+#define CF_CUDA(call, what)                              \
+    do {                                                 \
+        cudaError_t c_ = (call);                         \
+        if (c_ != cudaSuccess) return cuda_fail(e, c_, what); \
+    } while (0)
+

@@ -106,6 +106,58 @@ __global__ void __launch_bounds__(Geo<LG, R>::T, MinBlocks<LG>::v) k_suffix(KPar
     pr.run();
 }
 
+// ------------------------------------------------------------------------------------------
+// Work queue: one persistent launch over many (d, prime) tables of one transform length, each with
+// its own n, F, d, model and query list.  A CTA takes the next item from a device counter with an
+// atomic add (nothing waits on anything), runs it in its own workspace slot, and takes another
+// until the list is exhausted; the host orders the list heaviest first.
+// ------------------------------------------------------------------------------------------
+struct QItem {
+    u64 prime;
+    int n, F, d, model, J, q0;  // table size, factorial range, degree, model, queries [q0, q0 + J)
+};
+struct QueueParams {
+    const QItem* items;
+    int count;
+    int* next;                // next unclaimed item (zeroed before the launch)
+    const int* qn;            // [sum J] query sizes, by item
+    const int* qM;
+    const long long* qout;    // [sum J] output index of each query
+};
+template <int LG, int R, bool W>
+__global__ void __launch_bounds__(Geo<LG, R>::T, MinBlocks<LG>::v) k_suffix_queue(KParams kp, QueueParams qp) {
+    typedef Geo<LG, R> G;
+    typedef PrimeRun<G, DevExec<G>, W> PR;
+    extern __shared__ __align__(16) u64 smem[];
+    __shared__ __align__(16) unsigned char ikp_raw[sizeof(KParams)];  // the current item's parameters
+    KParams& ikp = *reinterpret_cast<KParams*>(ikp_raw);
+    __shared__ int item;
+    DevExec<G> ex;
+    u32* tm_slot = (u32*)(smem + Smem<G>::MISC + MI_TMEM);
+    if constexpr (PR::TM) ex.tmem_alloc(tm_slot);  // once for all the CTA's items
+    for (;;) {
+        if (threadIdx.x == 0) {
+            item = atomicAdd(qp.next, 1);
+            if (item < qp.count) {
+                const QItem& q = qp.items[item];
+                ikp = kp;
+                ikp.primes = &q.prime;
+                ikp.B = 1;
+                ikp.n = q.n, ikp.F = q.F, ikp.d = q.d, ikp.model = q.model, ikp.J = q.J;
+                ikp.d0 = q.model == MODEL_SUBSET ? q.d : 1;
+                ikp.qn = qp.qn + q.q0, ikp.qM = qp.qM + q.q0, ikp.qout = qp.qout + q.q0;
+            }
+        }
+        __syncthreads();
+        if (item >= qp.count) break;
+        PR pr(ex, ikp, 0, smem, (int)blockIdx.x);
+        pr.run_prime();
+        __syncthreads();  // ikp and item are rewritten for the next item
+    }
+    if constexpr (PR::TM) ex.tmem_free(*tm_slot);
+}
+typedef void (*qfn_t)(KParams, QueueParams);
+
 // Elements per thread (2^R): 32 at L = 2^10, 16 at L = 2^11 .. 2^14, fewer below so a CTA keeps at
 // least a warp.  R = 4 was measured on B200 against R = 5 (twice the threads): n = 2048: 1826 ->
 // 2244, n = 4096: 496 -> 540, n = 8192: 122 -> 170, n = 16384: 40.8 -> 48.5 prime-residues/s
@@ -119,14 +171,16 @@ typedef void (*kfn_t)(KParams);
 struct KInfo {
     kfn_t fn;
     int threads;
-    size_t smem;
-    int r;  // log2 of the entries per thread
+    size_t smem;  // fixed dynamic shared memory; a launch with J queries adds 8 J (threads / 32)
+    int r;        // log2 of the entries per thread
+    qfn_t qfn;    // the work-queue form
+    size_t smem_for(int J) const { return smem + (size_t)8 * J * (threads >= 32 ? threads / 32 : 1); }
 };
 // W selects the kernel for primes below 2^62 (otherwise below 2^50).
 template <int LG, bool W = false>
 inline KInfo kinfo() {
     typedef Geo<LG, RFor<LG>::R> G;
-    return KInfo{&k_suffix<LG, RFor<LG>::R, W>, G::T, Smem<G>::BYTES, RFor<LG>::R};
+    return KInfo{&k_suffix<LG, RFor<LG>::R, W>, G::T, Smem<G>::BYTES, RFor<LG>::R, &k_suffix_queue<LG, RFor<LG>::R, W>};
 }
 
 }  // namespace cfb

@@ -181,7 +181,14 @@ extern "C" int cf_residues_noalloc(const uint64_t* primes, int B, int nmax, int 
         cudaError_t c_ = (call);                                                                \
         if (c_ != cudaSuccess) return fail(CF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(c_)); \
     } while (0)
-    NA_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ki.smem), "shared memory attribute");
+    const size_t smem = ki.smem_for(J);
+    {
+        int dev = 0, optin = 0;
+        NA_CUDA(cudaGetDevice(&dev), "current device");
+        NA_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "shared memory limit");
+        if (smem > (size_t)optin) return fail(CF_ERR_UNSUPPORTED, std::to_string(J) + " queries exceed the shared memory of one block");
+    }
+    NA_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "shared memory attribute");
     NA_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), s), "error reset");
     if (J) {
         NA_CUDA(cudaMemcpyAsync(d_qn, qn, sizeof(int) * J, cudaMemcpyHostToDevice, s), "query upload");
@@ -206,7 +213,7 @@ extern "C" int cf_residues_noalloc(const uint64_t* primes, int B, int nmax, int 
         kp.lay = lay;
         kp.out = d_out;
         kp.err = d_err;
-        ki.fn<<<nb, ki.threads, ki.smem, s>>>(kp);
+        ki.fn<<<nb, ki.threads, smem, s>>>(kp);
         NA_CUDA(cudaGetLastError(), "kernel launch");
         if (J) NA_CUDA(cudaMemcpyAsync(residues + (size_t)at * J, d_out, 8 * (size_t)nb * J, cudaMemcpyDeviceToHost, s), "residue download");
     }

@@ -21,8 +21,10 @@
 //   * the powers g^p and g^-q of a step are running Montgomery products per thread (each thread
 //     holds the entries t + k T), started from a small per-step table of powers in shared memory;
 //   * the queries are evaluated on the fly from the stage-1 input rows (the same U[w] the
-//     reference's k_query builds), reduced per warp and stored per warp, so a batch needs no
-//     separate pass over V and no block barrier per row.
+//     reference's k_query builds), over the row's live entries only; each warp leaves its partial
+//     sum in shared memory and, after the transform's first barrier, one warp per query folds the
+//     row's partials into one word, so a batch needs no separate pass over V and no barrier of its
+//     own per row.
 //
 // The kernel code runs through an Exec policy: on the GPU `each` is the calling thread and
 // `sync` is __syncthreads; a CPU harness (tests) runs the same phases thread by thread.
@@ -229,7 +231,8 @@ CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R) {
     o.D = lay_take(at, 2 * ((size_t)n + 1));      // pairs: 1/k!^2
     for (int l = 0; l < 8; ++l) o.WL[l] = l < R ? lay_take(at, 2 * (((size_t)L >> (l + 1)) + 1)) : 0;  // pairs
     o.hat = lay_take(at, 2 * (size_t)L);          // pairs: spectrum of the kernel 1/t, times 1/L
-    o.ps = lay_take(at, (size_t)J * nw * (n + 1));  // [J][nw][n+1]
+    o.ps = lay_take(at, (size_t)J * (n + 1));  // [J][n+1] row sums per query
+    (void)nw;
     o.total = at;
     return o;
 }
@@ -262,8 +265,9 @@ struct KParams {
     u64* ws;            // workspace base
     size_t ws_words;    // words per prime
     Layout lay;         // offsets inside a prime's workspace
-    u64* out;           // [B][J] residues
+    u64* out;           // [B][J] residues, or out[qout[j]] when qout is set
     int* err;           // device error word (0 = ok)
+    const long long* qout = nullptr;  // [J] output index of each query (work-queue items), or null
     u64* keep = nullptr;  // resident tables [B][keep_words] (serving builds), or null
     size_t keep_words = 0;
 };
@@ -284,6 +288,10 @@ struct Smem {
     static constexpr int PW_STRIDE = 72;
     static constexpr int WORDS = PW + 2 * PW_STRIDE;
     static constexpr size_t BYTES = (size_t)WORDS * 8;
+    // [J][NW] per-warp query partial sums of the current row, after the fixed part (the launch's
+    // dynamic shared memory is BYTES + 8 J NW)
+    static constexpr int QS = WORDS;
+    static constexpr size_t bytes_for(int J) { return BYTES + (size_t)8 * J * G::NW; }
 };
 enum { MI_P = 0, MI_PINV = 1, MI_R1 = 2, MI_R2 = 3, MI_ONEQ = 4, MI_ROOT = 5, MI_LINV = 6, MI_TMEM = 7 };
 
@@ -315,9 +323,10 @@ struct PrimeRun {
     u64* sm;    // shared memory
     u64 P;
 
-    CF_HD PrimeRun(X& e, const KParams& k, int bi, u64* smem) : ex(e), kp(k), b(bi), sm(smem) {
+    // bi: the prime's index in kp.primes (and its output row); slot: its workspace slot (bi if < 0)
+    CF_HD PrimeRun(X& e, const KParams& k, int bi, u64* smem, int slot = -1) : ex(e), kp(k), b(bi), sm(smem) {
         P = kp.primes[b];
-        base = kp.ws + (size_t)b * kp.ws_words;
+        base = kp.ws + (size_t)(slot < 0 ? bi : slot) * kp.ws_words;
     }
     // workspace tables (offsets live in the kernel parameters, so these hold no registers)
     CF_HD u64* V() const { return base + kp.lay.V; }
@@ -743,7 +752,7 @@ struct PrimeRun {
         ex.each([&](int t, Regs<G>&) CF_INL {
             for (int k = t; k <= F; k += T) put_pair(inv(), k, k ? canon(sh(val(ifact(), k), fact(), k - 1)) : 0, P);
             for (int k = t; k <= n; k += T) put_pair(D(), k, canon(sh(val(ifact(), k), ifact(), k)), P);
-            const size_t nps = (size_t)J * NW * (n + 1);
+            const size_t nps = (size_t)J * (n + 1);
             for (size_t k = t; k < nps; k += T) ps()[k] = 0;
         });
         // a root of unity of order L: x^((p-1)/L) whose (L/2)-th power is -1 (fast/cuckoo_fast.cu:815-820)
@@ -860,33 +869,49 @@ struct PrimeRun {
     // ---------------------------------------------------------------------------------------
     // Query partial sums for row q: sum_{w<q} Vs[q][w] / (M_j - w) for every query with n_j >= q
     // (the U[w] / (M - w) sums of fast/cuckoo_fast.cu:306-323, 595-622).  The row is in the
-    // registers (layout 0, entries outside the row zero); each warp stores its own partial sum.
+    // registers (layout 0, entries outside the row zero).  Only the slots below q are visited: the
+    // warp leaves the unrolled slot loop at its first slot wholly at or above q (slot indices grow
+    // with j, so the exit is warp-uniform), which makes a query cost about n_j^2 / 2 products
+    // instead of n_j L.  Each warp leaves its sum at QS[j][warp] in shared memory; fold_queries
+    // combines them after the next barrier.
     // ---------------------------------------------------------------------------------------
     CF_HD void query_row(int q) {
+        u64* qs = sm + Smem<G>::QS;
         for (int jq = 0; jq < kp.J; ++jq) {
             const int nj = kp.qn[jq], Mj = kp.qM[jq];
             if (nj < q) continue;
             ex.each([&](int t, Regs<G>& rg) CF_INL {
-                const u64* iv = inv();
-                u64 acc = 0;
-                // 1/(M - w) for the slots' w (clamped to a valid entry outside the row)
-                pipe_pairs<E, PD, WK>(
-                    [&](auto jc) CF_INL {
-                        const int w = G::idx(0, t, decltype(jc)::value);
-                        return iv + 2 * (w < q ? Mj - w : Mj);
-                    },
-                    [&](auto jc, u64 c, u64 cq) CF_INL {
-                        constexpr int j = decltype(jc)::value;
-                        if (G::idx(0, t, j) < q) {
-                            if constexpr (W) acc = madd(acc, canon(shoup_mul_lazy(rg.x[j], c, cq, P)), P);
-                            else acc += shoup_mul_lazy(rg.x[j], c, cq, P);  // < 2^57
-                        }
-                    },
-                    [&](auto) CF_INL { pin(acc); });
+                const u64* iv = inv() + 2 * (size_t)Mj;  // the pair of 1/(M_j - w) sits at iv - 2w
+                const int tw = t & ~31;                  // the warp's first thread
+                u64 acc = 0, c0 = 0, q0 = 0;
+                if (G::idx(0, t, 0) < q) ld_pair(iv - 2 * G::idx(0, t, 0), c0, q0);
+#pragma unroll
+                for (int j = 0; j < E; ++j) {
+                    const bool more = j + 1 < E && G::idx(0, tw, j + 1) < q;
+                    u64 c1 = 0, q1 = 0;  // slots at or above q multiply by zero
+                    if (more && G::idx(0, t, j + 1) < q) ld_pair(iv - 2 * G::idx(0, t, j + 1), c1, q1);
+                    if constexpr (W) acc = madd(acc, canon(shoup_mul_lazy(rg.x[j], c0, q0, P)), P);
+                    else acc += shoup_mul_lazy(rg.x[j], c0, q0, P);  // E terms below 4p: < 2^57
+                    if (!more) break;
+                    c0 = c1, q0 = q1;
+                }
                 const u64 part = canon(shoup_mul_lazy(acc, 1, misc()[MI_ONEQ], P));
-                ex.warp_sum_store(t, part, P, ps() + (size_t)jq * NW * (kp.n + 1) + q, (size_t)(kp.n + 1));
+                ex.warp_sum_store(t, part, P, qs + (size_t)jq * NW, 1);
             });
         }
+    }
+    // Row q's per-warp partials (written by query_row before a barrier) into ps[j][q]: warp w folds
+    // queries w, w + NW, ... with shuffles.
+    CF_HD void fold_queries(int q) {
+        const u64* qs = sm + Smem<G>::QS;
+        ex.each([&](int t, Regs<G>&) CF_INL {
+            const int w = t >> 5, lane = t & 31;
+            for (int jq = w; jq < kp.J; jq += NW) {
+                if (kp.qn[jq] < q) continue;
+                const u64 v = lane < NW ? qs[(size_t)jq * NW + lane] : 0;
+                ex.warp_sum_store(t, v, P, ps() + (size_t)jq * (kp.n + 1) + q, 0);
+            }
+        });
     }
 
     // One step of the suffix recurrence (fast/cuckoo_fast.cu:841-855).
@@ -920,6 +945,7 @@ struct PrimeRun {
                     },
                     [&](auto jc) CF_INL { pin(rg.x[decltype(jc)::value]); });
             });
+            fold_queries(v);  // after the transform's barriers: every warp's partial of row v is in
         }
         if (v >= d0) {  // stage 2: column v of V from row v of S
             ex.sync();  // column v of S is read below
@@ -1050,6 +1076,8 @@ struct PrimeRun {
         if (n > d0) {  // the last row n for queries with n_j = n
             ex.each([&](int t, Regs<G>& rg) CF_INL { load_row(t, rg.x, V(), VS(), n, d0, n); });
             query_row(n);
+            ex.sync();
+            fold_queries(n);
         }
         ex.sync();
         for (int jq = 0; jq < kp.J; ++jq) {
@@ -1059,11 +1087,10 @@ struct PrimeRun {
                 u64 Qm;
                 if (kp.model == MODEL_REPLACEMENT) Qm = mont_pow(to_mont((u64)Mj, m), (u64)kp.d, m);
                 else Qm = to_mont(canon(sh(sh(val(fact(), Mj), ifact(), kp.d), ifact(), Mj - kp.d)), m);
-                const u64* pst = ps() + (size_t)jq * NW * (n + 1);
+                const u64* pst = ps() + (size_t)jq * (n + 1);
                 u64 acc = 0;
                 for (int k = t + 1; k <= nj; k += T) {
-                    u64 y = 0;
-                    for (int w = 0; w < NW; ++w) y = madd(y, pst[(size_t)w * (n + 1) + k], P);
+                    u64 y = pst[k];
                     y = sh(y, inv(), k);
                     y = sh(y, ifact(), nj - k);
                     y = sh(y, ifact(), Mj - k);
@@ -1074,16 +1101,28 @@ struct PrimeRun {
                 red[t] = acc;
             });
             const u64 s = sum_red();
-            ex.single([&]() CF_INL { kp.out[(size_t)b * kp.J + jq] = canon(sh(canon(sh(s, fact(), nj)), fact(), Mj)); });
+            ex.single([&]() CF_INL {
+                kp.out[kp.qout ? (size_t)kp.qout[jq] : (size_t)b * kp.J + jq] = canon(sh(canon(sh(s, fact(), nj)), fact(), Mj));
+            });
         }
     }
 
-    CF_HD void run() {
+    // Tensor memory for the kernel spectrum is taken once per CTA, around all the primes it runs.
+    CF_HD void acquire() {
         if constexpr (TM) ex.tmem_alloc((u32*)(misc() + MI_TMEM));
+    }
+    CF_HD void release() {
+        if constexpr (TM) ex.tmem_free((u32)misc()[MI_TMEM]);
+    }
+    CF_HD void run_prime() {
         setup();
         for (int v = 1; v < kp.n; ++v) step(v);
         finish();
-        if constexpr (TM) ex.tmem_free((u32)misc()[MI_TMEM]);
+    }
+    CF_HD void run() {
+        acquire();
+        run_prime();
+        release();
     }
 };
 

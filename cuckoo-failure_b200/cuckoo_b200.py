@@ -97,6 +97,24 @@ def lib():
         L.cf_batch_graph_launches.restype = ctypes.c_long
         L.cf_batch_graph_destroy.argtypes = [ctypes.c_void_p]
         L.cf_batch_graph_destroy.restype = None
+        L.cf_uneven_create.argtypes = [ctypes.c_void_p, _intp, _intp, _intp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.POINTER(ctypes.c_void_p)]
+        L.cf_uneven_create.restype = ctypes.c_int
+        for f in (L.cf_uneven_outputs, L.cf_uneven_tables, L.cf_uneven_launches):
+            f.argtypes = [ctypes.c_void_p]
+            f.restype = ctypes.c_long
+        L.cf_uneven_offset.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.cf_uneven_offset.restype = ctypes.c_long
+        L.cf_uneven_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.cf_uneven_launch.restype = ctypes.c_int
+        L.cf_uneven_results.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_void_p]
+        L.cf_uneven_results.restype = ctypes.c_int
+        L.cf_uneven_destroy.argtypes = [ctypes.c_void_p]
+        L.cf_uneven_destroy.restype = None
+        L.cf_uneven_describe.argtypes = [_intp, _intp, _intp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_long,
+                                         ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.POINTER(ctypes.c_long),
+                                         ctypes.c_long]
+        L.cf_uneven_describe.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -194,6 +212,10 @@ class Engine:
         """Build and keep the suffix tables of `primes` on the device for later queries."""
         return Tables(self, primes, nmax, Fmax, d, model)
 
+    def uneven(self, instances, model=MODEL_SUBSET, bits=50, first=0, count=-1, stride=1):
+        """Plan and capture an uneven batch over instances [(n, M, d)] (cf_uneven_create)."""
+        return Uneven(self, instances, model, bits, first, count, stride)
+
     def max_batch(self, nmax, Mmax, J):
         return int(lib().cf_max_batch(self._h, nmax, Mmax, J))
 
@@ -245,6 +267,77 @@ class BatchGraph:
 
     def __exit__(self, *a):
         self.close()
+
+
+def _instance_arrays(instances):
+    n = np.ascontiguousarray([x[0] for x in instances], dtype=np.int32)
+    M = np.ascontiguousarray([x[1] for x in instances], dtype=np.int32)
+    d = np.ascontiguousarray([x[2] for x in instances], dtype=np.int32)
+    return n, M, d
+
+
+class Uneven:
+    """An uneven batch captured as one CUDA graph (one work-queue launch per transform length):
+    launch() replays it, results() returns [residues of instance k modulo its primes 0 .. need - 1]."""
+
+    def __init__(self, engine, instances, model=MODEL_SUBSET, bits=50, first=0, count=-1, stride=1):
+        self.instances = [tuple(int(v) for v in x) for x in instances]
+        n, M, d = _instance_arrays(self.instances)
+        h = ctypes.c_void_p()
+        rc = lib().cf_uneven_create(engine._h, n.ctypes.data_as(_intp), M.ctypes.data_as(_intp),
+                                    d.ctypes.data_as(_intp), len(n), model, bits, first, count, stride, ctypes.byref(h))
+        engine._check(rc)
+        self._u = h
+        self.outputs = int(lib().cf_uneven_outputs(h))
+        self.offsets = [int(lib().cf_uneven_offset(h, k)) for k in range(len(n))] + [self.outputs]
+
+    def tables(self):
+        return int(lib().cf_uneven_tables(self._u))
+
+    def launches(self):
+        return int(lib().cf_uneven_launches(self._u))
+
+    def launch(self, stream_ptr=None):
+        rc = lib().cf_uneven_launch(self._u, ctypes.c_void_p(stream_ptr or 0))
+        if rc != CF_OK:
+            raise EngineError(rc, "uneven batch launch failed")
+
+    def results(self, stream_ptr=None):
+        out = np.zeros(max(self.outputs, 1), dtype=np.uint64)
+        rc = lib().cf_uneven_results(self._u, out.ctypes.data_as(_u64p), ctypes.c_void_p(stream_ptr or 0))
+        if rc != CF_OK:
+            raise EngineError(rc, "uneven batch failed its device checks")
+        return [out[self.offsets[k]:self.offsets[k + 1]] for k in range(len(self.instances))]
+
+    def close(self):
+        if getattr(self, "_u", None):
+            lib().cf_uneven_destroy(self._u)
+            self._u = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def uneven_describe(instances, model=MODEL_SUBSET, bits=50, first=0, count=-1, stride=1, jcap=0):
+    """The plan of an uneven batch without a device: [(d, prime index, lg, n, F, J, q0)] in launch order."""
+    n, M, d = _instance_arrays(instances)
+    args = (n.ctypes.data_as(_intp), M.ctypes.data_as(_intp), d.ctypes.data_as(_intp), len(n), model, bits, first,
+            count, stride, jcap)
+    k = int(lib().cf_uneven_describe(*args, None, 0))
+    if k < 0:
+        raise ValueError("invalid instances")
+    buf = (ctypes.c_long * (7 * max(k, 1)))()
+    lib().cf_uneven_describe(*args, buf, k)
+    return [tuple(buf[7 * t:7 * t + 7]) for t in range(k)]
 
 
 class Tables:

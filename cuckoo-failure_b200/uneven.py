@@ -28,3 +28,46 @@ def instances(count=512, seed=CONFIG4_SEED, n_lo=256, n_hi=16384, m_mult=(2, 3, 
         d = int(rng.choice(d_choices))
         out.append((n, M, d))
     return out
+
+
+def tables(instances, need, first=0, count=-1, stride=1):
+    """The (d, prime) tables of an uneven batch, restated from the reference's driver rule: per d,
+    prime i serves the instances of that d with i < need, and its table is built to their largest n
+    (fast/cuckoo_fast.cu:787-795, 859-866).  need(n, M, d) gives the primes an instance needs.
+    Returns {(d, i): [instance indices]} for the planned prime indices first + j stride."""
+    out = {}
+    needs = [need(n, M, d) for n, M, d in instances]
+    top = max(needs) if count < 0 else min(first + count, max(needs))
+    for d in sorted({x[2] for x in instances}):
+        ks = [k for k, x in enumerate(instances) if x[2] == d]
+        for i in range(first, top, stride):
+            act = [k for k in ks if i < needs[k]]
+            if act:
+                out[(d, i)] = act
+    return out
+
+
+def run(engine, instances, model=0, bits=50, first=0, count=-1, stride=1, stream_ptr=None):
+    """Residues of every instance through one uneven-batch graph: [array over the instance's primes]
+    (entries of prime indices left out of a sampled plan stay zero)."""
+    with engine.uneven(instances, model, bits, first, count, stride) as u:
+        u.launch(stream_ptr)
+        return u.results(stream_ptr)
+
+
+def per_instance(engine, instances, prime_range, need, model=0, first=0, count=-1, stride=1):
+    """The plain form: every instance alone, one table per prime at its own n (one cf_residues call,
+    a launch per chunk of primes, per instance), over the same planned prime indices."""
+    out = []
+    for n, M, d in instances:
+        k = need(n, M, d)
+        top = k if count < 0 else min(first + count, k)
+        idx = list(range(first, top, stride))
+        res = [0] * k
+        if idx:
+            ps = prime_range(0, top)
+            r = engine.residues([ps[i] for i in idx], n, d, [(n, M)], model=model)
+            for i, v in zip(idx, r[:, 0]):
+                res[i] = int(v)
+        out.append(res)
+    return out

@@ -132,6 +132,38 @@ int cf_tables_query(cf_engine* e, const cf_tables* t, const int* qn, const int* 
 int cf_tables_count(const cf_tables* t);
 void cf_tables_free(cf_tables* t);
 
+/* ---- uneven batches: many instances in one graph of work-queue launches ----
+ * Instances k = 0 .. K-1, (n[k], M[k], d[k]) under one model and prime list (bits = 50 or 62):
+ * instance k needs N_bad(n[k], M[k]) modulo primes 0 .. need_k - 1 of the list, written at
+ * residues[off_k + i] with off_k = cf_uneven_offset(u, k) (the prefix sums of the needs).  One table
+ * per (d, prime index) serves every instance of degree d that needs the prime, built to the largest
+ * such n: the reference's rule for a batch of primes (fast/cuckoo_fast.cu:787-795, 859-866) applied
+ * per prime.  The tables are grouped by transform length; each group is one persistent launch whose
+ * CTAs take tables heaviest first from a device counter; the groups are captured as one CUDA graph.
+ * Only prime indices first + j stride < first + count are planned (count < 0: all), the rest of
+ * the residues are left zero; a sampled plan times a whole workload on part of its primes.
+ * Instances need 1 <= n < M, n <= 16384, and d <= M for the subset model.
+ * The reference runs one instance set per process and d (fast/cuckoo_fast.cu:648-904). */
+typedef struct cf_uneven cf_uneven;
+int cf_uneven_create(cf_engine* e, const int* n, const int* M, const int* d, int K, int model, int bits, long first,
+                     long count, long stride, cf_uneven** out);
+/* Words of the residue array (the sum of the needs), instance k's offset in it, tables planned,
+ * kernel launches per replay. */
+long cf_uneven_outputs(const cf_uneven* u);
+long cf_uneven_offset(const cf_uneven* u, int k);
+long cf_uneven_tables(const cf_uneven* u);
+long cf_uneven_launches(const cf_uneven* u);
+/* Replay the graph on `stream` (NULL: the default stream); returns without waiting. */
+int cf_uneven_launch(cf_uneven* u, void* stream);
+/* Wait for `stream`, copy all residues to the host buffer; CF_ERR_DEVICE if a device check failed. */
+int cf_uneven_results(cf_uneven* u, uint64_t* residues, void* stream);
+void cf_uneven_destroy(cf_uneven* u);
+/* The plan without a device (tests, tooling): rows of 7 longs per table, in launch order:
+ * d, prime index, log2 transform length, table n, F, queries J, first query.  jcap > 0 splits tables
+ * with more queries.  Returns the number of tables (writing at most cap rows), -1 on bad input. */
+long cf_uneven_describe(const int* n, const int* M, const int* d, int K, int model, int bits, long first, long count,
+                        long stride, int jcap, long* tables, long cap);
+
 /* ---- allocation-free variant (no counterpart in the reference) ---- */
 
 /* Bytes of the static device scratch used by cf_residues_noalloc (64 MiB).  One prime's table

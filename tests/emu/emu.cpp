@@ -52,10 +52,11 @@ struct HostExec {
     }
     void tmem_wait_ld() {}
     void tmem_wait_st() {}
-    // warp sums, as on the device: threads of a warp run one after another, dst starts at zero
+    // warp sums, as on the device: threads of a warp run one after another, lane 0 first, so lane 0
+    // stores and the later lanes add (the destination's old contents never count)
     void warp_sum_store(int t, u64 v, u64 P, u64* dst, size_t stride) {
         u64* c = dst + (size_t)(t >> 5) * stride;
-        *c = madd(*c, v, P);
+        *c = (t & 31) == 0 ? v : madd(*c, v, P);
     }
     void reduce_mod(u64* red, int T, u64 P) {
         u64 s = 0;
@@ -72,7 +73,7 @@ struct RFor {
 template <int LG, bool W>
 static int run_lg(const KParams& kp) {
     typedef Geo<LG, RFor<LG>::R> G;
-    std::vector<u64> smem(Smem<G>::WORDS);
+    std::vector<u64> smem(Smem<G>::bytes_for(kp.J) / 8, 0xA5A5A5A5A5A5A5A5ull);
     for (int b = 0; b < kp.B; ++b) {
         HostExec<G> ex;
         PrimeRun<G, HostExec<G>, W> pr(ex, kp, b, smem.data());
@@ -159,4 +160,72 @@ static int emu_run(const uint64_t* primes, int B, int nmax, int d, int model, co
         return -6;  // a value bound of the transforms did not hold (check_bound)
     }
     return err ? -5 : 0;
+}
+
+// ---- uneven batches: the work-queue launch's per-table semantics on the CPU ----
+// Each table of the plan (uneven_plan.hpp) runs with its own n, F, d, model and query list in a
+// workspace slot laid out for the largest table of its transform length (as k_suffix_queue's
+// slots are), freshly poisoned, and scatters its residues through the query output indices.
+#include "../../cuckoo-failure_b200/csrc/uneven_plan.hpp"
+
+template <int LG, bool W>
+static void run_table(const KParams& kp) {
+    typedef Geo<LG, RFor<LG>::R> G;
+    std::vector<u64> smem(Smem<G>::bytes_for(kp.J) / 8, 0xA5A5A5A5A5A5A5A5ull);
+    HostExec<G> ex;
+    PrimeRun<G, HostExec<G>, W> pr(ex, kp, 0, smem.data(), 0);
+    pr.acquire();
+    pr.run_prime();
+    pr.release();
+}
+
+extern "C" int emu_uneven(const int* n, const int* M, const int* d, int K, int model, int bits, long first, long count,
+                          long stride, uint64_t* out) {
+    cfh::UnevenPlan pl;
+    if (!cfh::plan_uneven(n, M, d, K, model, bits, first, count, stride, 0, pl)) return -1;
+    const bool wide = bits == 62;
+    int gn[16] = {0}, gF[16] = {0}, gJ[16] = {0};  // largest table of each transform length
+    for (const cfh::UnevenTable& t : pl.tables) {
+        gn[t.lg] = gn[t.lg] > t.n ? gn[t.lg] : t.n;
+        gF[t.lg] = gF[t.lg] > t.F ? gF[t.lg] : t.F;
+        gJ[t.lg] = gJ[t.lg] > t.J ? gJ[t.lg] : t.J;
+    }
+    int err = 0;
+    try {
+        for (const cfh::UnevenTable& t : pl.tables) {
+            const int R = (t.lg >= 11 && t.lg <= 14) ? 4 : (t.lg >= 10 ? 5 : (t.lg >= 6 ? t.lg - 5 : 1)), T = 1 << (t.lg - R);
+            const Layout lo = make_layout(gn[t.lg], gF[t.lg], 1 << t.lg, gJ[t.lg], T >= 32 ? T / 32 : 1, R);
+            std::vector<u64> ws(lo.total, 0xA5A5A5A5A5A5A5A5ull);
+            KParams kp;
+            kp.primes = &t.prime;
+            kp.B = 1;
+            kp.n = t.n, kp.F = t.F, kp.d = t.d, kp.model = model, kp.J = t.J;
+            kp.d0 = model == MODEL_SUBSET ? t.d : 1;
+            kp.qn = pl.qn.data() + t.q0, kp.qM = pl.qM.data() + t.q0, kp.qout = pl.qout.data() + t.q0;
+            kp.ws = ws.data();
+            kp.ws_words = lo.total;
+            kp.lay = lo;
+            kp.out = out;
+            kp.err = &err;
+            switch (t.lg) {
+                case 4: wide ? run_table<4, true>(kp) : run_table<4, false>(kp); break;
+                case 5: wide ? run_table<5, true>(kp) : run_table<5, false>(kp); break;
+                case 6: wide ? run_table<6, true>(kp) : run_table<6, false>(kp); break;
+                case 7: wide ? run_table<7, true>(kp) : run_table<7, false>(kp); break;
+                case 8: wide ? run_table<8, true>(kp) : run_table<8, false>(kp); break;
+                case 9: wide ? run_table<9, true>(kp) : run_table<9, false>(kp); break;
+                case 10: wide ? run_table<10, true>(kp) : run_table<10, false>(kp); break;
+                case 11: wide ? run_table<11, true>(kp) : run_table<11, false>(kp); break;
+                default: return -4;  // larger lengths are too slow for CPU tests
+            }
+        }
+    } catch (const std::runtime_error&) {
+        return -6;
+    }
+    return err ? -5 : 0;
+}
+extern "C" long emu_uneven_outputs(const int* n, const int* M, const int* d, int K, int model, int bits) {
+    cfh::UnevenPlan pl;
+    if (!cfh::plan_uneven(n, M, d, K, model, bits, 0, 0, 1, 0, pl)) return -1;
+    return pl.outputs;
 }
