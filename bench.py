@@ -132,6 +132,37 @@ def run_reference_wave(binary, n, M, d, first, procs):
     return dt, [ln for o in outs for ln in o.splitlines()]
 
 
+def reference_gpu(n, M, d, primes=64, timeout_s=900):
+    """The reference's CUDA build (fast/cuckoo_fast.cu compiled by its own `fast-gpu` recipe, with an
+    sm_100a target: oracle/Makefile.ref) on this GPU: primes 0 .. primes-1 in one run, its default
+    batch (at most 64 primes, fast/cuckoo_fast.cu:743-747).  The rate is over the run's own clock
+    up to its queries done (setup, uploads, the step loop, k_query, download, Horner finish), which
+    leaves out only process start and CUDA context creation; its residues for primes 0 and 1 are
+    checked against the reference host build's."""
+    import re
+
+    binary = os.path.join(REF_DIR, "cuckoo_fast_gpu")
+    if not os.path.exists(binary):
+        return None
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(f"{n} {M}\n")
+        qpath = f.name
+    t0 = time.perf_counter()
+    r = subprocess.run([binary, str(d), qpath, "0", str(primes)], capture_output=True, text=True, timeout=timeout_s)
+    wall = time.perf_counter() - t0
+    os.unlink(qpath)
+    if r.returncode:
+        return {"unavailable": f"exit {r.returncode}: {r.stderr.strip()[-200:]}"}
+    m = re.search(r"build done at ([0-9.]+) s, queries at ([0-9.]+) s", r.stderr)
+    got = {int(t[0]): int(t[4]) for t in (ln.split() for ln in r.stdout.splitlines()) if len(t) == 5}
+    for i, want in golden_check(n, M, d).items():
+        assert got.get(i) == want, f"reference CUDA build: residue mismatch at prime {i}"
+    done = float(m.group(2)) if m else wall
+    return {"value": primes / done, "unit": UNIT, "primes": primes, "build_done_s": float(m.group(1)) if m else None,
+            "queries_done_s": done, "wall_s": wall,
+            "what": "the reference's CUDA build on this GPU, one run over primes 0..%d at n=%d, M=%d, d=%d" % (primes - 1, n, M, d)}
+
+
 def cpu_baseline(n, M, d):
     binary, kind = reference_binary()
     P = host_cores()
@@ -195,6 +226,93 @@ def serving_run(device, seconds, rate=200.0, n_lo=64, n_hi=2048, budget_gb=150.0
                     "1.07 GB per prime, 14184 primes at d = 3); such requests take the plain path"}
 
 
+def timed_replays(launch, stream, reps):
+    """Device time (ms) of `reps` back-to-back calls of launch(stream_ptr) on `stream`, after one warm-up."""
+    import torch
+
+    launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        launch(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def uneven_run(eng, stride, per_instance_count=32, seed=None):
+    """The uneven-batch workload (512 instances: n log-uniform in [256, 16384], M = n U{2, 3, 4},
+    d in {2, 3, 4}, seed-fixed), every instance modulo its own need(n, M, d) primes, on the prime
+    indices that are multiples of `stride` (a sample whose tables follow the whole run's mix).
+    Timed as one graph of work-queue launches, beside the plain form: each instance alone, one
+    cf_residues call (a launch per chunk of primes) per instance, on the first per_instance_count
+    instances and the same prime indices."""
+    import numpy as np
+    import torch
+
+    import cuckoo_b200 as cb
+    import uneven
+
+    insts = uneven.instances(512, seed=seed or uneven.CONFIG4_SEED)
+    needs = [cb.need(n, M, d) for n, M, d in insts]
+    planned = [len(range(0, k, stride)) for k in needs]
+    stream = torch.cuda.Stream()
+    with eng.uneven(insts, stride=stride) as u:
+        ms = timed_replays(u.launch, stream, 1)
+        res = u.results(stream.cuda_stream)
+        tables, launches = u.tables(), u.launches()
+    full_tables = len(cb.uneven_describe(insts))
+    sub = insts[:per_instance_count]
+    t0 = time.perf_counter()
+    alone = uneven.per_instance(eng, sub, cb.prime_range, cb.need, stride=stride)
+    plain_s = time.perf_counter() - t0
+    for k in range(len(sub)):  # the same residues both ways
+        assert [int(x) for x in res[k][::stride]] == alone[k][::stride], f"uneven instance {k} differs"
+    sub_residues = sum(planned[:per_instance_count])
+    sub_share = sub_residues / max(1, sum(planned))
+    return {"workload": "512 instances, n log-uniform [256, 16384], M = n U{2,3,4}, d U{2,3,4}, "
+                        f"seed {uneven.CONFIG4_SEED}; prime indices i = 0 mod {stride} of each instance's need",
+            "tables": tables, "tables_full_run": full_tables, "launches_per_graph": launches,
+            "instance_residues": sum(planned), "ms": ms,
+            "instance_residues_per_s": sum(planned) / (ms * 1e-3), "tables_per_s": tables / (ms * 1e-3),
+            "full_run_s_est": full_tables / (tables / (ms * 1e-3)),
+            "per_instance_form": {"instances": per_instance_count, "instance_residues": sub_residues,
+                                  "s": plain_s, "instance_residues_per_s": sub_residues / plain_s,
+                                  "full_run_s_est": plain_s / sub_share,
+                                  "what": "each instance alone: one cf_residues call over its planned primes, its own n"}}
+
+
+def sweep_run(eng, n, M, B, reps=2):
+    """Config-3 sweep at n = 16384, M = 2n: d = 2 and 4 (subset model) and the replacement model at
+    d = 3, one graph-captured 148-prime launch per step, the residues of primes 0 and 1 checked
+    where the reference has them."""
+    import numpy as np
+    import torch
+
+    import cuckoo_b200 as cb
+
+    out = {}
+    stream = torch.cuda.Stream()
+    for d, model in ((2, cb.MODEL_SUBSET), (4, cb.MODEL_SUBSET), (3, cb.MODEL_REPLACEMENT)):
+        primes = cb.prime_range(0, B)
+        d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
+        d_out = torch.empty(B, dtype=torch.int64, device="cuda")
+        g = eng.batch_graph(d_primes.data_ptr(), B, n, d, [(n, M)], d_out.data_ptr(), model=model)
+        ms = timed_replays(g.launch, stream, reps)
+        g.status(stream.cuda_stream)
+        g.close()
+        got = d_out.cpu().numpy().view(np.uint64)
+        if model == cb.MODEL_SUBSET:
+            for i, r in golden_check(n, M, d).items():
+                assert int(got[i]) == r, f"d={d}: residue mismatch at prime {i}"
+        key = f"d{d}" + ("_replacement" if model else "")
+        out[key] = {"value": B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": reps,
+                    "primes_needed": cb.need(n, M, d, model),
+                    "frac": B * algorithmic_mm(n) * K_OPS_PER_MM / (ms * 1e-3) / 1e12}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -211,6 +329,11 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the served-query latency run")
     ap.add_argument("--no-plain-form", action="store_true", help="skip the one-prime-per-launch timing")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch (512 instances) run")
+    ap.add_argument("--uneven-stride", type=int, default=97)
+    ap.add_argument("--no-sweep", action="store_true", help="skip d = 2, 4 and the replacement model")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="--impl reference: skip the reference's CUDA build (timed beside its host build)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the main kernel from an ncu capture (roofline.traffic)")
     a = ap.parse_args()
@@ -236,6 +359,7 @@ def main():
                 times.append(dt)
         tot = sum(times)
         v = P * a.steps / tot
+        rgpu = reference_gpu(n, M, d) if not a.no_reference_gpu else None
         print(json.dumps({
             "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1e3 * tot / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -243,7 +367,8 @@ def main():
             "config": {"workload": workload, "batch_primes_per_step": P, "l2": "inputs larger than L2"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": P, "kind": "reference",
                              "sample": f"each step {P} processes x 1 prime with the reference's {kind}"},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu": rgpu}))
         return 0
 
     import ctypes
@@ -352,12 +477,22 @@ def main():
         gbs = traffic / (ms / a.steps * 1e-3) / 1e9
         peak_gbs, which = hbm_peak()
         hbm = {"achieved": gbs, "peak": peak_gbs, "unit": "GB/s", "frac": gbs / peak_gbs, "peak_source": which}
+    eng.close()  # its workspace (a wave of tables) goes back before the runs below allocate theirs
+    sweep = None
+    if rank == 0 and world == 1 and not a.no_sweep and n == 16384:
+        with cb.Engine(local) as eng2:
+            sweep = sweep_run(eng2, n, M, B)
+        for v in sweep.values():
+            v["frac"] = v["frac"] / peak if peak else None
+    unev = None
+    if rank == 0 and world == 1 and not a.no_uneven:
+        with cb.Engine(local) as eng2:
+            unev = uneven_run(eng2, a.uneven_stride)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(reference_binary()[0]):
         cpu = cpu_baseline(n, M, d)
     serving = None
     if rank == 0 and world == 1 and not a.no_serving:
-        eng.close()  # release the build workspace: the resident tables need the memory
         serving = serving_run(local, a.serve_seconds)
     if rank == 0:
         print(json.dumps({
@@ -372,7 +507,7 @@ def main():
                          "model": f"{K_OPS_PER_MM} INT32 multiply ops per modular multiplication, "
                                   f"{algorithmic_mm(n):.3e} multiplications per prime-residue; peak measured live"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-            "plain_form": plain, "serving": serving}))
+            "plain_form": plain, "config3_sweep": sweep, "uneven": unev, "serving": serving}))
     if dist:
         dist.destroy_process_group()
     return 0

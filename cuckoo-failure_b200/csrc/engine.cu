@@ -139,8 +139,11 @@ int check_smem(cf_engine* e, size_t smem, int J) {
 }
 
 // fixed_ws: use the workspace as it is (a graph capture, where nothing may be allocated)
+// err: the device error word the launch reports to (the engine's unless given)
 static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int d, int model, int J, const Plan& pl,
-                        u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0, bool fixed_ws = false) {
+                        u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0, bool fixed_ws = false,
+                        int* err = nullptr) {
+    if (!err) err = e->d_err;
     const KInfo ki = kernel_for(pl.lg, pl.wide);
     if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     const size_t smem = ki.smem_for(J);
@@ -160,7 +163,8 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
         if (rc) return rc;
         cap = want;
     }
-    CF_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(int), s), "error reset");
+    if (e->max_ctas > 0) cap = std::min<long>(cap, e->max_ctas);
+    CF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s), "error reset");
     // equal chunks: a short tail launch would cost as much time as a full one
     const long nchunks = (B + cap - 1) / cap, per = (B + nchunks - 1) / nchunks;
     for (int at = 0; at < B; at += (int)per) {
@@ -180,7 +184,7 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
         kp.ws_words = pl.ws_words;
         kp.lay = pl.lay;
         kp.out = d_out + (size_t)at * J;
-        kp.err = e->d_err;
+        kp.err = err;
         kp.keep = keep ? keep + (size_t)at * keep_words : nullptr;
         kp.keep_words = keep_words;
         ki.fn<<<nb, ki.threads, smem, s>>>(kp);
@@ -273,9 +277,12 @@ struct cf_tables {
     size_t keep_words = 0;
     u64* d_primes = nullptr;
     std::vector<u64> primes;
-    u64* d_out = nullptr;  // [B][jcap] query results
-    int* d_q = nullptr;    // [2][jcap]
+    u64* d_out = nullptr;  // [B][jcap] results of the waiting query form
     int jcap = 0;
+    int* d_err = nullptr;     // the build's device error word
+    int* h_err = nullptr;     // its pinned host copy, written when the build is done
+    cudaEvent_t built = nullptr;
+    bool pooled = false;      // keep / d_primes from the stream-ordered allocator
 };
 
 uint64_t cf_tables_bytes(int nmax, int Fmax) {
@@ -283,8 +290,11 @@ uint64_t cf_tables_bytes(int nmax, int Fmax) {
     return 8 * make_keep_layout(nmax, std::max(nmax, Fmax)).total;
 }
 
-int cf_tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int Fmax, int d, int model, cf_tables** out) {
-    if (!e || !out) return CF_ERR_ARG;
+// The build of both forms: memory, the persistent launch with the table set's own error word, the
+// error word's copy to the host and the `built` event, all on stream s; no wait.  The stream-ordered
+// form (pooled) allocates and frees on streams, so neither blocks the device.
+static int tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int Fmax, int d, int model,
+                        cudaStream_t s, bool pooled, cf_tables** out) {
     *out = nullptr;
     e->err.clear();
     e->launches = 0;
@@ -303,22 +313,27 @@ int cf_tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int F
     t->device = e->device, t->n = nmax, t->F = pl.F, t->d = d, t->d0 = pl.d0, t->model = model, t->B = B;
     t->keep_words = make_keep_layout(nmax, pl.F).total;
     t->primes.assign(primes, primes + B);
-    cudaError_t c = cudaMalloc(&t->keep, 8 * t->keep_words * (size_t)B);
-    if (c == cudaSuccess) c = cudaMalloc(&t->d_primes, 8 * (size_t)B);
-    if (c == cudaSuccess) c = cudaMemcpyAsync(t->d_primes, primes, 8 * (size_t)B, cudaMemcpyHostToDevice, e->stream);
+    t->pooled = pooled;
+    const size_t kb = 8 * t->keep_words * (size_t)B;
+    cudaError_t c = pooled ? cudaMallocAsync(&t->keep, kb, s) : cudaMalloc(&t->keep, kb);
+    if (c == cudaSuccess) c = pooled ? cudaMallocAsync(&t->d_primes, 8 * (size_t)B, s) : cudaMalloc(&t->d_primes, 8 * (size_t)B);
+    if (c == cudaSuccess) c = cudaMalloc(&t->d_err, sizeof(int));
+    if (c == cudaSuccess) c = cudaHostAlloc(&t->h_err, sizeof(int), cudaHostAllocDefault);
+    if (c == cudaSuccess) c = cudaEventCreateWithFlags(&t->built, cudaEventDisableTiming);
+    if (c == cudaSuccess) c = cudaMemcpyAsync(t->d_primes, primes, 8 * (size_t)B, cudaMemcpyHostToDevice, s);
     if (c != cudaSuccess) {
         cf_tables_free(t);
         return cuda_fail(e, c, "resident table allocation");
     }
-    rc = launch_batch(e, t->d_primes, B, nmax, d, model, 0, pl, nullptr, e->stream, t->keep, t->keep_words);
+    *t->h_err = -1;  // not done
+    rc = launch_batch(e, t->d_primes, B, nmax, d, model, 0, pl, nullptr, s, t->keep, t->keep_words, false, t->d_err);
     if (rc == CF_OK) {
-        int herr = 0;
-        c = cudaMemcpyAsync(&herr, e->d_err, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
-        if (c == cudaSuccess) c = cudaStreamSynchronize(e->stream);
+        c = cudaMemcpyAsync(t->h_err, t->d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (c == cudaSuccess) c = cudaEventRecord(t->built, s);
         if (c != cudaSuccess) rc = cuda_fail(e, c, "table build");
-        else if (herr) rc = fail(e, CF_ERR_DEVICE, "device check failed (code " + std::to_string(herr) + ")");
     }
     if (rc) {
+        cudaStreamSynchronize(s);
         cf_tables_free(t);
         return rc;
     }
@@ -326,45 +341,91 @@ int cf_tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int F
     return CF_OK;
 }
 
-int cf_tables_query(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, uint64_t* residues) {
-    if (!e || !t) return CF_ERR_ARG;
-    e->err.clear();
-    e->launches = 0;
-    if (J < 1 || !qn || !qM || !residues) return fail(e, CF_ERR_ARG, "bad query buffers");
+int cf_tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int Fmax, int d, int model, cf_tables** out) {
+    if (!e || !out) return CF_ERR_ARG;
+    int rc = tables_build(e, primes, B, nmax, Fmax, d, model, e->stream, false, out);
+    if (rc) return rc;
+    CF_CUDA(cudaEventSynchronize((*out)->built), "table build");
+    if (*(*out)->h_err) {
+        const int herr = *(*out)->h_err;
+        cf_tables_free(*out);
+        *out = nullptr;
+        return fail(e, CF_ERR_DEVICE, "device check failed (code " + std::to_string(herr) + ")");
+    }
+    return CF_OK;
+}
+
+int cf_tables_build_async(cf_engine* e, const uint64_t* primes, int B, int nmax, int Fmax, int d, int model, void* stream,
+                          cf_tables** out) {
+    if (!e || !out) return CF_ERR_ARG;
+    return tables_build(e, primes, B, nmax, Fmax, d, model, (cudaStream_t)stream, true, out);
+}
+
+int cf_tables_ready(const cf_tables* t) {
+    if (!t || !t->built) return CF_ERR_ARG;
+    if (cudaSetDevice(t->device) != cudaSuccess) return CF_ERR_CUDA;
+    const cudaError_t c = cudaEventQuery(t->built);
+    if (c == cudaErrorNotReady) return 0;
+    if (c != cudaSuccess) return CF_ERR_CUDA;
+    return *t->h_err ? CF_ERR_DEVICE : 1;
+}
+
+// Residues of the queries into d_residues[b * J + j] on stream s, as launches of up to TQ_MAXJ
+// queries whose sizes travel in the kernel parameters; no wait.
+static int tables_query(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, u64* d_out, cudaStream_t s) {
+    if (J < 1 || !qn || !qM || !d_out) return fail(e, CF_ERR_ARG, "bad query buffers");
     for (int j = 0; j < J; ++j) {
         if (qn[j] < 1 || qn[j] > t->n || qM[j] <= qn[j] || qM[j] > t->F)
             return fail(e, CF_ERR_ARG, "query needs 1 <= n <= table n and n < M <= table F");
         if (t->model == CF_MODEL_SUBSET && t->d > qM[j]) return fail(e, CF_ERR_ARG, "subset model needs d <= M");
     }
-    CF_CUDA(cudaSetDevice(t->device), "set device");
-    cf_tables* tm = const_cast<cf_tables*>(t);  // the query staging buffers are per table set
-    if (J > tm->jcap) {
-        cudaFree(tm->d_out);
-        cudaFree(tm->d_q);
-        tm->d_out = nullptr;
-        tm->d_q = nullptr;
-        tm->jcap = 0;
-        CF_CUDA(cudaMalloc(&tm->d_out, 8 * (size_t)t->B * J), "query result buffer");
-        CF_CUDA(cudaMalloc(&tm->d_q, sizeof(int) * 2 * (size_t)J), "query buffer");
-        tm->jcap = J;
-    }
-    cudaStream_t s = e->stream;
-    CF_CUDA(cudaMemcpyAsync(tm->d_q, qn, sizeof(int) * J, cudaMemcpyHostToDevice, s), "query upload");
-    CF_CUDA(cudaMemcpyAsync(tm->d_q + J, qM, sizeof(int) * J, cudaMemcpyHostToDevice, s), "query upload");
-    TQParams tp;
-    tp.primes = t->d_primes;
-    tp.B = t->B, tp.n = t->n, tp.F = t->F, tp.d = t->d, tp.d0 = t->d0, tp.model = t->model, tp.J = J;
-    tp.qn = tm->d_q;
-    tp.qM = tm->d_q + J;
-    tp.keep = t->keep;
-    tp.keep_words = t->keep_words;
-    tp.out = tm->d_out;
     const size_t smem = tq_smem_bytes(t->n);
     CF_CUDA(cudaFuncSetAttribute((const void*)k_table_query<TQ_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
             "shared memory attribute");
-    k_table_query<TQ_THREADS><<<t->B * J, TQ_THREADS, smem, s>>>(tp);
-    CF_CUDA(cudaGetLastError(), "query launch");
-    ++e->launches;
+    for (int j0 = 0; j0 < J; j0 += TQ_MAXJ) {
+        TQParams tp;
+        tp.primes = t->d_primes;
+        tp.B = t->B, tp.n = t->n, tp.F = t->F, tp.d = t->d, tp.d0 = t->d0, tp.model = t->model;
+        tp.J = std::min(TQ_MAXJ, J - j0);
+        for (int j = 0; j < tp.J; ++j) tp.qn[j] = qn[j0 + j], tp.qM[j] = qM[j0 + j];
+        tp.keep = t->keep;
+        tp.keep_words = t->keep_words;
+        tp.out = d_out + j0;
+        tp.out_stride = (size_t)J;
+        k_table_query<TQ_THREADS><<<t->B * tp.J, TQ_THREADS, smem, s>>>(tp);
+        CF_CUDA(cudaGetLastError(), "query launch");
+        ++e->launches;
+    }
+    return CF_OK;
+}
+
+int cf_tables_query_async(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, uint64_t* d_residues,
+                          void* stream) {
+    if (!e || !t) return CF_ERR_ARG;
+    e->err.clear();
+    e->launches = 0;
+    CF_CUDA(cudaSetDevice(t->device), "set device");
+    return tables_query(e, t, qn, qM, J, d_residues, (cudaStream_t)stream);
+}
+
+int cf_tables_query(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, uint64_t* residues) {
+    if (!e || !t) return CF_ERR_ARG;
+    e->err.clear();
+    e->launches = 0;
+    if (J < 1 || !qn || !qM || !residues) return fail(e, CF_ERR_ARG, "bad query buffers");
+    CF_CUDA(cudaSetDevice(t->device), "set device");
+    cf_tables* tm = const_cast<cf_tables*>(t);  // the waiting form's result buffer is per table set
+    if (J > tm->jcap) {
+        cudaFree(tm->d_out);
+        tm->d_out = nullptr;
+        tm->jcap = 0;
+        CF_CUDA(cudaMalloc(&tm->d_out, 8 * (size_t)t->B * J), "query result buffer");
+        tm->jcap = J;
+    }
+    cudaStream_t s = e->stream;
+    CF_CUDA(cudaStreamWaitEvent(s, t->built, 0), "wait for the build");
+    int rc = tables_query(e, t, qn, qM, J, tm->d_out, s);
+    if (rc) return rc;
     CF_CUDA(cudaMemcpyAsync(residues, tm->d_out, 8 * (size_t)t->B * J, cudaMemcpyDeviceToHost, s), "query download");
     CF_CUDA(cudaStreamSynchronize(s), "query");
     return CF_OK;
@@ -375,11 +436,24 @@ int cf_tables_count(const cf_tables* t) { return t ? t->B : 0; }
 void cf_tables_free(cf_tables* t) {
     if (!t) return;
     cudaSetDevice(t->device);
-    cudaFree(t->keep);
-    cudaFree(t->d_primes);
+    if (t->pooled) {  // back to the pool in stream order, without waiting for the device
+        cudaFreeAsync(t->keep, 0);
+        cudaFreeAsync(t->d_primes, 0);
+    } else {
+        cudaFree(t->keep);
+        cudaFree(t->d_primes);
+    }
     cudaFree(t->d_out);
-    cudaFree(t->d_q);
+    cudaFree(t->d_err);
+    if (t->h_err) cudaFreeHost(t->h_err);
+    if (t->built) cudaEventDestroy(t->built);
     delete t;
+}
+
+int cf_engine_set_max_ctas(cf_engine* e, int n) {
+    if (!e || n < 0) return CF_ERR_ARG;
+    e->max_ctas = n;
+    return CF_OK;
 }
 
 long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J) {

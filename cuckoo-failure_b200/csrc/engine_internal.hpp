@@ -56,6 +56,7 @@ struct cf_engine {
     int jcap = 0;
     long launches = 0;
     int prime_bits = 50;  // for cf_residues_async, whose primes are not read on the host
+    int max_ctas = 0;     // CTAs (primes) per launch at most, 0 = no cap
     std::string err;
 };
 

@@ -147,6 +147,21 @@ CF_HD u64 shoup_mul_lazy(u64 a, u64 w, u64 wq, u64 p) {
 #endif
 }
 
+// Shoup companion floor(w 2^64 / p) for w < p from three per-prime constants: mu = floor(2^64 / p),
+// r = 2^64 mod p and rq = floor(r 2^64 / p).  Since w 2^64 = w mu p + w r, the companion is
+// w mu + floor(w r / p); the second term is the quotient of a Shoup product by r, whose lazy
+// estimate (shoup_mul_lazy's) is at most 3 low and is corrected against the remainder.  Every sum
+// is below 2^64, so arithmetic modulo 2^64 is exact.  Replaces the 64-step division in hot code.
+CF_HD u64 shoup_companion_fast(u64 w, u64 p, u64 mu, u64 r, u64 rq) {
+    const u32 a0 = lo32(w), a1 = hi32(w), q0 = lo32(rq), q1 = hi32(rq);
+    u64 q = wmul(a1, q1) + (wmul(a0, q1) >> 32) + (wmul(a1, q0) >> 32);
+    u64 rem = w * r - q * p;  // the true remainder, below 4p
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (rem >= p) rem -= p, ++q;
+    return w * mu + q;
+}
+
 // a w mod p in [0, 2p) for any 64-bit a, given w < p and wq = floor(w 2^64 / p).
 CF_HD u64 shoup_mul(u64 a, u64 w, u64 wq, const Mod& md) {
     const u32 a0 = lo32(a), a1 = hi32(a), q0 = lo32(wq), q1 = hi32(wq);

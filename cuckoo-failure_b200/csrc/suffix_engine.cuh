@@ -129,6 +129,25 @@ CF_HD void pipe_pairs(A&& addr, F&& apply, Dn&& done) {
         },
         done);
 }
+// The same over the slots for which live(IC<J>) holds (a warp-uniform test): the others issue
+// neither their constant load nor their unit.
+template <int N, int D, int K, class Lv, class A, class F, class Dn>
+CF_HD void pipe_pairs_live(Lv&& live, A&& addr, F&& apply, Dn&& done) {
+    u64 ra[D + 1] = {}, rb[D + 1] = {};
+    window<D, 0>([&](auto jc) CF_INL {
+        constexpr int j = decltype(jc)::value;
+        if constexpr (j < N)
+            if (live(jc)) ld_pair(addr(jc), ra[j], rb[j]);
+    }, [&](auto) CF_INL {});
+    window<N, K>(
+        [&](auto jc) CF_INL {
+            constexpr int j = decltype(jc)::value;
+            if constexpr (j + D < N)
+                if (live(IC<j + D>{})) ld_pair(addr(IC<j + D>{}), ra[(j + D) % (D + 1)], rb[(j + D) % (D + 1)]);
+            if (live(jc)) apply(jc, ra[j % (D + 1)], rb[j % (D + 1)]);
+        },
+        done);
+}
 #ifndef CF_PIPE_D
 #define CF_PIPE_D 4
 #endif
@@ -209,7 +228,7 @@ CF_HD size_t blk_off(int r, int c, int h) {
 // Per-prime global workspace, in 64-bit words (every table 256-byte aligned).
 // Tables marked "pairs" hold (value, Shoup companion) interleaved: entry k at [2k], [2k+1].
 struct Layout {
-    size_t V, S, VS, SS, fact, ifact, inv, D, hat, ps, total;
+    size_t V, S, VS, SS, fact, ifact, inv, D, Gm, hat, ps, total;
     size_t WL[8];  // pass-0 twiddles by level: WL[s] holds pairs w^(u 2^s), u = 0 .. L/2^(s+1)
 };
 CF_HD size_t lay_take(size_t& at, size_t cnt) {
@@ -229,6 +248,7 @@ CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R) {
     o.ifact = lay_take(at, 2 * ((size_t)F + 1));  // pairs: 1/k!
     o.inv = lay_take(at, 2 * ((size_t)F + 1));    // pairs: 1/k
     o.D = lay_take(at, 2 * ((size_t)n + 1));      // pairs: 1/k!^2
+    o.Gm = lay_take(at, 2 * ((size_t)n + 1));     // (g(v), 1/g(v)) in Montgomery form, v = 0 .. n
     for (int l = 0; l < 8; ++l) o.WL[l] = l < R ? lay_take(at, 2 * (((size_t)L >> (l + 1)) + 1)) : 0;  // pairs
     o.hat = lay_take(at, 2 * (size_t)L);          // pairs: spectrum of the kernel 1/t, times 1/L
     o.ps = lay_take(at, (size_t)J * (n + 1));  // [J][n+1] row sums per query
@@ -285,7 +305,7 @@ struct Smem {
     static constexpr int TWS_N = (G::L >> (G::R + 1)) + 1;
     // [2][PW_STRIDE] powers of 1/g(v) and g(v) for stage 2, rebuilt every step (power_tables)
     static constexpr int PW = TWS + 2 * TWS_N;
-    static constexpr int PW_STRIDE = 72;
+    static constexpr int PW_STRIDE = 104;
     static constexpr int WORDS = PW + 2 * PW_STRIDE;
     static constexpr size_t BYTES = (size_t)WORDS * 8;
     // [J][NW] per-warp query partial sums of the current row, after the fixed part (the launch's
@@ -293,7 +313,11 @@ struct Smem {
     static constexpr int QS = WORDS;
     static constexpr size_t bytes_for(int J) { return BYTES + (size_t)8 * J * G::NW; }
 };
-enum { MI_P = 0, MI_PINV = 1, MI_R1 = 2, MI_R2 = 3, MI_ONEQ = 4, MI_ROOT = 5, MI_LINV = 6, MI_TMEM = 7 };
+enum { MI_P = 0, MI_PINV = 1, MI_R1 = 2, MI_R2 = 3, MI_ONEQ = 4, MI_ROOT = 5, MI_LINV = 6, MI_TMEM = 7, MI_R1Q = 8 };
+// Slots of a power table (power_tables): h^k at PW_A + k (k < TA), h^(TA k) at PW_B + k (k < TB),
+// h^(T j) at PW_J + j (j < E), the chains' step h^(NCH T) as a plain residue and its Shoup companion
+// at PW_STEP, PW_STEPQ, and h^L at PW_L.
+enum { PW_A = 0, PW_B = 32, PW_J = 64, PW_STEP = 96, PW_STEPQ = 97, PW_L = 98 };
 
 template <class G>
 struct Regs {
@@ -309,6 +333,7 @@ template <class G, class X, bool W = false>
 struct PrimeRun {
     static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP, NW = G::NW;
     static_assert(W || G::LG <= 14, "reduction-free forward transform needs 2^LG p < 2^64");
+    static_assert(NP > 1, "layout 0 must hold index t + jT in slot j of thread t");
     // L = 2^14 (1024 threads x 16 entries): the kernel spectrum lives in tensor memory, each
     // thread's 16 (value, companion) pairs in its own 64 columns (all 512 columns of the SM's 128
     // lanes); smaller transforms, several CTAs to an SM, read it from global.
@@ -337,6 +362,7 @@ struct PrimeRun {
     CF_HD u64* ifact() const { return base + kp.lay.ifact; }
     CF_HD u64* inv() const { return base + kp.lay.inv; }
     CF_HD u64* D() const { return base + kp.lay.D; }
+    CF_HD u64* Gm() const { return base + kp.lay.Gm; }
     CF_HD u64* WL(int l) const { return base + kp.lay.WL[l]; }
     CF_HD u64* tws() const { return sm + Smem<G>::TWS; }
     CF_HD u64* hat() const { return base + kp.lay.hat; }
@@ -352,9 +378,11 @@ struct PrimeRun {
     CF_HD u64 sh(u64 a, const u64* pairs, int k) const {  // a * pairs[k], result in [0, 4p)
         return shoup_mul_lazy(a, CF_LDG(pairs + 2 * k), CF_LDG(pairs + 2 * k + 1), P);
     }
-    CF_HD static void put_pair(u64* pairs, int k, u64 v, u64 P) {
+    // Shoup companion of w < p, from the per-prime constants setup keeps in shared memory
+    CF_HD u64 companion(u64 w) const { return shoup_companion_fast(w, P, misc()[MI_ONEQ], misc()[MI_R1], misc()[MI_R1Q]); }
+    CF_HD void put_pair(u64* pairs, int k, u64 v) const {
         pairs[2 * k] = v;
-        pairs[2 * k + 1] = shoup_companion(v, P);
+        pairs[2 * k + 1] = companion(v);
     }
     CF_HD u64 canon(u64 x) const { return red2(red2(x, 2 * P), P); }  // [0, 4p) -> [0, p)
 
@@ -426,7 +454,9 @@ struct PrimeRun {
     template <int PASS, bool FWD>
     CF_HD void pass(int t, u64 (&x)[E]) const {
         typedef Plan<PASS, FWD> PL;
-        constexpr int D = PD;
+        // pass 0 reads its twiddles from L2 (the others from shared memory): at 1024 threads it
+        // prefetches them two groups ahead (72.1 against 70.3 prime-residues/s at n = 16384)
+        constexpr int D = (PASS == 0 && T >= 1024) ? 2 : PD;
         const int off = PL::bb ? (t & ((1 << PL::bb) - 1)) : 0;
         const u64 P4 = 4 * P, P2 = 2 * P;
         u64 rw[D + 1], rq[D + 1];
@@ -626,37 +656,43 @@ struct PrimeRun {
     // one another are NCH times fewer than with one chain.
     static constexpr int NCH = E >= 4 ? 4 : E;
 
-    // Stage-2 powers of h = 1/g(v) (row load) and h = g(v) (products), Montgomery form.  Rather
-    // than an exponentiation per thread, the CTA builds at the start of each step a two-level
-    // table per base in shared memory: A[k] = h^k (k < TA = min(T, 32)) at slots 0.., B[k] =
-    // h^(TA k) (k < TB = T / TA) at slots 32.., h^T and h^L at slots 64 and 66, and the chains'
-    // step h^(NCH T) as a plain residue with its Shoup companion at slots 65 and 67 (a Shoup
-    // product by it keeps a Montgomery-form power in Montgomery form).  Thread t starts its
-    // chains from A[t % TA] B[t / TA].  The 2 (TA + TB + 3) entries are independent
-    // exponentiations; task k runs on lane k / NW of warp k % NW, so every warp takes a few and
-    // none lags at the next barrier.
+    // Stage-2 powers of h = 1/g(v) (base 0: the row products) and h = g(v) (base 1: the stage-2
+    // products), Montgomery form, rebuilt at the start of each step in shared memory (the PW_*
+    // slots): A[k] = h^k (k < TA = min(T, 32)), B[k] = h^(TA k) (k < TB = T / TA), J[j] = h^(T j)
+    // (j < E), the chains' step h^(NCH T) as a plain residue with its Shoup companion (a Shoup product
+    // by it keeps a Montgomery-form power in Montgomery form), and h^L.  Slot j of thread t holds
+    // index t + jT, whose power is A[t % TA] B[t / TA] J[j].  The six groups (A, B, J for two bases)
+    // go to six warps, fewer warps looping over them; a group's lanes raise a common base (h, h^TA
+    // or h^T, which every lane squares up itself) to their own small exponent, so the deepest chain
+    // is about 20 products, and h comes from the table of g(v) built at setup.  The other warps go
+    // straight on with stage 1: the tables are read only after its barriers.
     static constexpr int TA = T < 32 ? T : 32, TB = T / TA;
-    static constexpr int PW_TASKS = 2 * (TA + TB + 3);
+    static constexpr int LW = T < 32 ? T : 32;  // lanes of a warp
+    CF_HD static constexpr int log2c(int x) { return x <= 1 ? 0 : 1 + log2c(x / 2); }
     CF_HD void power_tables(int v) {
         u64* pw = sm + Smem<G>::PW;
+        const u64* gm = Gm();
         ex.each([&](int t, Regs<G>&) CF_INL {
-            const Mod m = md();
-            for (int k = (t & 31) * NW + (t >> 5); k < PW_TASKS; k += T) {
-                const int base = k < PW_TASKS / 2 ? 0 : 1, r = k - base * (PW_TASKS / 2);
-                const u64 h = base ? g_mont(v, m) : ginv_mont(v, m);
-                u64 e;
-                int slot;
-                if (r < TA) e = (u64)r, slot = r;
-                else if (r < TA + TB) e = (u64)TA * (r - TA), slot = 32 + r - TA;
-                else if (r == TA + TB) e = (u64)T, slot = 64;
-                else if (r == TA + TB + 1) e = (u64)NCH * T, slot = 65;
-                else e = (u64)L, slot = 66;
-                u64 y = mont_pow(h, e, m);
-                if (slot == 65) {
-                    y = from_mont(y, m);
-                    pw[base * Smem<G>::PW_STRIDE + 67] = shoup_companion(y, P);
+            const int lane = t & 31;
+            for (int gi = t >> 5; gi < 6; gi += NW) {
+                const int base = gi & 1, kind = gi >> 1;
+                const int size = kind == 0 ? TA : kind == 1 ? TB : E + 2;
+                if (lane >= size) continue;
+                const Mod m = md();
+                u64* tab = pw + base * Smem<G>::PW_STRIDE;
+                u64 b = CF_LDG(gm + 2 * v + 1 - base);  // 1/g(v) or g(v)
+                const int sq = kind == 0 ? 0 : kind == 1 ? log2c(TA) : log2c(T);
+                for (int i = 0; i < sq; ++i) b = mont_mul(b, b, m);
+                for (int k = lane; k < size; k += LW) {
+                    if (kind == 0) tab[PW_A + k] = mont_pow(b, (u64)k, m);
+                    else if (kind == 1) tab[PW_B + k] = mont_pow(b, (u64)k, m);
+                    else if (k < E) tab[PW_J + k] = mont_pow(b, (u64)k, m);
+                    else if (k == E) {
+                        const u64 y = from_mont(mont_pow(b, (u64)NCH, m), m);
+                        tab[PW_STEP] = y;
+                        tab[PW_STEPQ] = shoup_companion_fast(y, P, misc()[MI_ONEQ], m.r1, misc()[MI_R1Q]);
+                    } else tab[PW_L] = mont_pow(b, (u64)E, m);
                 }
-                pw[base * Smem<G>::PW_STRIDE + slot] = y;
             }
         });
     }
@@ -668,23 +704,29 @@ struct PrimeRun {
         if constexpr (W) return canon(y);
         return y;
     }
-    CF_HD void power_chains(int base, int t, const Mod& m, u64 (&f)[NCH], u64& step, u64& stepq) const {
+    // Chains started at slot j0 (the first slot a warp needs): chain c starts at the first slot
+    // j >= j0 with j = c (mod NCH), from A[t % TA] B[t / TA] J[j].
+    CF_HD void power_chains(int base, int t, const Mod& m, u64 (&f)[NCH], u64& step, u64& stepq, int j0 = 0) const {
         const u64* pw = sm + Smem<G>::PW + base * Smem<G>::PW_STRIDE;
-        f[0] = TB > 1 ? mont_mul(pw[t % TA], pw[32 + t / TA], m) : pw[t];
-        const u64 hT = pw[64];
-        for (int c = 1; c < NCH; ++c) f[c] = mont_mul(f[c - 1], hT, m);
-        step = pw[65], stepq = pw[67];
+        const u64 ab = TB > 1 ? mont_mul(pw[PW_A + t % TA], pw[PW_B + t / TA], m) : pw[PW_A + t];
+#pragma unroll
+        for (int c = 0; c < NCH; ++c) {
+            const int jc = j0 + ((c - j0) & (NCH - 1));
+            f[c] = jc == 0 ? ab : (jc < E ? mont_mul(ab, pw[PW_J + jc], m) : 0);
+        }
+        step = pw[PW_STEP], stepq = pw[PW_STEPQ];
+    }
+    // Index range [lo, hi] of slot j (layout 0: index t + jT) over the calling thread's warp: the
+    // stage loops skip a slot, warp-uniformly, when no lane of the warp needs it.
+    CF_HD static void warp_slot_range(int t, int j, int& lo, int& hi) {
+        const int tw = t & ~31;
+        lo = tw + j * T;
+        hi = (T < 32 ? T - 1 : tw + 31) + j * T;
     }
 
-    // g(v) and 1/g(v) in Montgomery form (g != 0 for v >= d0)
-    CF_HD u64 g_mont(int v, const Mod& m) const {
-        if (kp.model == MODEL_REPLACEMENT) return mont_pow(to_mont((u64)v, m), (u64)kp.d, m);
-        return to_mont(canon(sh(sh(val(fact(), v), ifact(), kp.d), ifact(), v - kp.d)), m);  // C(v, d)
-    }
-    CF_HD u64 ginv_mont(int v, const Mod& m) const {
-        if (kp.model == MODEL_REPLACEMENT) return mont_pow(to_mont(val(inv(), v), m), (u64)kp.d, m);
-        return to_mont(canon(sh(sh(val(ifact(), v), fact(), kp.d), fact(), v - kp.d)), m);
-    }
+    // g(v) and 1/g(v) in Montgomery form, from the table built at setup (0 for v < d0, subset model)
+    CF_HD u64 g_mont(int v) const { return CF_LDG(Gm() + 2 * v); }
+    CF_HD u64 ginv_mont(int v) const { return CF_LDG(Gm() + 2 * v + 1); }
 
     // ---------------------------------------------------------------------------------------
     // Setup: factorials, inverses, D, twiddles and the kernel spectrum of 1/t (the per-batch host
@@ -698,6 +740,7 @@ struct PrimeRun {
             const Mod m = make_mod(P);
             mi[MI_P] = m.p, mi[MI_PINV] = m.pinv, mi[MI_R1] = m.r1, mi[MI_R2] = m.r2;
             mi[MI_ONEQ] = shoup_companion(1, P);
+            mi[MI_R1Q] = shoup_companion(m.r1, P);
         });
         ex.sync();
         const int C = (F + 1 + T - 1) / T;  // factorial entries k = 0..F, chunk of C per thread
@@ -739,19 +782,35 @@ struct PrimeRun {
                     run = mont_mul(run, km, m);
                     km = madd(km, m.r1, P);
                 }
-                put_pair(fact(), k, from_mont(run, m), P);
+                put_pair(fact(), k, from_mont(run, m));
             }
             run = red[T + t];  // 1/(k1 - 1)!
             for (int k = k1 - 1; k >= k0; --k) {  // 1/(k-1)! = k / k!
-                put_pair(ifact(), k, from_mont(run, m), P);
+                put_pair(ifact(), k, from_mont(run, m));
                 if (k > 0) run = mont_mul(run, to_mont((u64)k, m), m);
             }
         });
         ex.sync();
         // inv[k] = (k-1)!/k!, D[k] = 1/k!^2, Kq[k] = companion of k; query partial sums zeroed
         ex.each([&](int t, Regs<G>&) CF_INL {
-            for (int k = t; k <= F; k += T) put_pair(inv(), k, k ? canon(sh(val(ifact(), k), fact(), k - 1)) : 0, P);
-            for (int k = t; k <= n; k += T) put_pair(D(), k, canon(sh(val(ifact(), k), ifact(), k)), P);
+            for (int k = t; k <= F; k += T) put_pair(inv(), k, k ? canon(sh(val(ifact(), k), fact(), k - 1)) : 0);
+            for (int k = t; k <= n; k += T) put_pair(D(), k, canon(sh(val(ifact(), k), ifact(), k)));
+            // g(k) and 1/g(k), Montgomery form: C(k, d) and its inverse, or k^d and (1/k)^d
+            const Mod m = md();
+            for (int k = t; k <= n; k += T) {
+                u64 g = 0, gi = 0;
+                if (kp.model == MODEL_REPLACEMENT) {
+                    if (k > 0) {
+                        g = mont_pow(to_mont((u64)k, m), (u64)kp.d, m);
+                        gi = mont_pow(to_mont(inv()[2 * k], m), (u64)kp.d, m);  // this thread wrote inv[k]
+                    }
+                } else if (k >= kp.d) {
+                    g = to_mont(canon(sh(sh(val(fact(), k), ifact(), kp.d), ifact(), k - kp.d)), m);
+                    gi = to_mont(canon(sh(sh(val(ifact(), k), fact(), kp.d), fact(), k - kp.d)), m);
+                }
+                Gm()[2 * k] = g;
+                Gm()[2 * k + 1] = gi;
+            }
             const size_t nps = (size_t)J * (n + 1);
             for (size_t k = t; k < nps; k += T) ps()[k] = 0;
         });
@@ -779,7 +838,7 @@ struct PrimeRun {
             u64 cur = mont_pow(w, (u64)t, m);
             const u64 step = mont_pow(w, (u64)T, m);
             for (int k = t; k <= L / 2; k += T) {  // w^k into every table that holds it
-                const u64 c = from_mont(cur, m), cq = shoup_companion(c, P);
+                const u64 c = from_mont(cur, m), cq = companion(c);
                 for (int l = 0; l < G::R && (k & ((1 << l) - 1)) == 0; ++l) {
                     u64* d = WL(l) + 2 * (k >> l);
                     d[0] = c, d[1] = cq;
@@ -814,7 +873,7 @@ struct PrimeRun {
         }
         ex.each([&](int t, Regs<G>& rg) CF_INL {
             const u64 linv = mi[MI_LINV];
-            const u64 linvq = shoup_companion(linv, P);
+            const u64 linvq = companion(linv);
             if constexpr (TM) {
                 const u32 ta = X::tmem_addr((u32)mi[MI_TMEM], t);
 #pragma unroll
@@ -822,7 +881,7 @@ struct PrimeRun {
                     u32 v[16];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        const u64 h = canon(shoup_mul_lazy(rg.x[4 * c + k], linv, linvq, P)), hq = shoup_companion(h, P);
+                        const u64 h = canon(shoup_mul_lazy(rg.x[4 * c + k], linv, linvq, P)), hq = companion(h);
                         v[4 * k] = lo32(h), v[4 * k + 1] = hi32(h), v[4 * k + 2] = lo32(hq), v[4 * k + 3] = hi32(hq);
                     }
                     ex.tmem_st16(t, ta + 16 * c, v);
@@ -830,7 +889,7 @@ struct PrimeRun {
                 ex.tmem_wait_st();
             } else {
 #pragma unroll
-                for (int j = 0; j < E; ++j) put_pair(hat(), G::idx(NP - 1, t, j), canon(shoup_mul_lazy(rg.x[j], linv, linvq, P)), P);
+                for (int j = 0; j < E; ++j) put_pair(hat(), G::idx(NP - 1, t, j), canon(shoup_mul_lazy(rg.x[j], linv, linvq, P)));
             }
         });
         ex.sync();
@@ -928,7 +987,12 @@ struct PrimeRun {
                 const u64 iv = val(inv(), v), ivq = CF_LDG(inv() + 2 * v + 1);
                 u64* col = SS() + (size_t)(v - tile_v0(v)) * (n + 1);  // S[.][v], by row
                 const u64* Dt = D();
-                pipe_pairs<E, PD, WK>(
+                pipe_pairs_live<E, PD, WK>(
+                    [&](auto jc) CF_INL {  // rows v .. n-1 of column v: slots where the warp holds one
+                        int lo, hi;
+                        warp_slot_range(t, decltype(jc)::value, lo, hi);
+                        return hi >= v && lo < n;
+                    },
                     [&](auto jc) CF_INL {
                         const int i = G::idx(0, t, decltype(jc)::value);
                         return Dt + 2 * (i >= v && i < n ? i - v : 0);
@@ -958,6 +1022,9 @@ struct PrimeRun {
                 window<E, WK>(
                     [&](auto jc) CF_INL {
                         constexpr int j = decltype(jc)::value;
+                        int lo, hi;
+                        warp_slot_range(t, j, lo, hi);
+                        if (lo > v) return;  // entries q <= v only: this slot and the later ones stay zero
                         pin(rg.x[j]);
                         rg.x[j] = mont_mul(rg.x[j], f[j % NCH], m);  // x, f < 4p: exact, canonical
                         f[j % NCH] = chain_step(f[j % NCH], step, stepq);
@@ -967,17 +1034,56 @@ struct PrimeRun {
             convolve();
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const Mod m = md();
+                // Entries p = v+1 .. n: the warp's first slot holding one is j0, and its chains start
+                // there.  When L = n, e[n] sits at index 0 (thread 0, slot 0): a slot of its own, done
+                // below by thread 0 alone when warp 0 skips slot 0, so no warp does more than the rest.
+                int j0 = 0;
+#pragma unroll
+                for (int j = 0; j < E; ++j) {
+                    int lo, hi;
+                    warp_slot_range(t, j, lo, hi);
+                    j0 += hi <= v;
+                }
                 u64 f[NCH], step, stepq;  // g^(t + jT)
-                power_chains(1, t, m, f, step, stepq);
+                power_chains(1, t, m, f, step, stepq, j0);
                 const u64 dv = val(D(), v);
                 u64* col = VS() + (size_t)(v - tile_v0(v)) * (n + 1);  // V[.][v], by row
                 const u64* Dt = D();
                 const u64 mu = misc()[MI_ONEQ];  // floor(2^64 / p)
-                const u64 fwrap = sm[Smem<G>::PW + Smem<G>::PW_STRIDE + 66];  // g^L, for e[n] at index 0 when L = n
+                const u64 fwrap = sm[Smem<G>::PW + Smem<G>::PW_STRIDE + PW_L];  // g^L, for e[n] at index 0 when L = n
                 // W: the multipliers p of the slots as a running Montgomery form (p = t + j T)
-                u64 pm = W ? to_mont((u64)t, m) : 0;
+                u64 pm = W ? to_mont((u64)(t + j0 * T), m) : 0;
                 const u64 pmT = W ? to_mont((u64)T, m) : 0, pmL = (W && t == 0 && n == L) ? to_mont((u64)L, m) : 0;
-                pipe_pairs<E, PD, WK>(
+                // V[p][v] = g^p D[p-v-1] (D[v] - p e[p]) for a conv output x = e[p], (c, cq) = D[p-v-1],
+                // gp = g^p and (W) pmv = p in Montgomery form
+                auto entry = [&](u64 x, int p, u64 c, u64 cq, u64 gp, u64 pmv) CF_INL {
+                    if constexpr (W) {  // x < 2P and pmv < P keep the product exact below 2^126
+                        const u64 pe = mont_mul(x, pmv, m);  // p e[p], canonical
+                        const u64 y = canon(shoup_mul_lazy(dv + P - pe, c, cq, P));
+                        return mont_mul(y, gp, m);
+                    } else {
+                        // p e[p]: with p floor(2^64/p) for the companion the quotient estimate loses
+                        // at most p x / 2^64 < INV_OUT more (x < INV_OUT P, p <= 2^14, P < 2^50),
+                        // so pe < (INV_OUT + 4) P
+                        (void)pmv;
+                        const u64 pe = shoup_mul_lazy(x, (u64)p, (u64)p * mu, P);
+                        check_bound(pe, G::INV_OUT + 4);
+                        const u64 y = shoup_mul_lazy(dv + (G::INV_OUT + 4) * P - pe, c, cq, P);
+                        return mont_mul(y, gp, m);
+                    }
+                };
+                const bool wrap0 = n == L && t == 0;  // this thread holds e[n] at index 0
+                if (wrap0 && j0 > 0 && L > v) {
+                    u64 c, cq;
+                    ld_pair(Dt + 2 * (L - v - 1), c, cq);
+                    st_stream(col + L, entry(rg.x[0], L, c, cq, fwrap, pmL));
+                }
+                pipe_pairs_live<E, PD, WK>(
+                    [&](auto jc) CF_INL {
+                        int lo, hi;
+                        warp_slot_range(t, decltype(jc)::value, lo, hi);
+                        return decltype(jc)::value >= j0 && lo <= n;
+                    },
                     [&](auto jc) CF_INL {
                         const int i = G::idx(0, t, decltype(jc)::value), p = i == 0 ? L : i;
                         return Dt + 2 * (p > v && p <= n ? p - v - 1 : 0);
@@ -989,19 +1095,7 @@ struct PrimeRun {
                         const int p = wrap ? L : i;
                         pin(rg.x[j]);
                         if (p > v && p <= n) {
-                            if constexpr (W) {  // x < 2P and pm < P keep the product exact below 2^126
-                                const u64 pe = mont_mul(rg.x[j], wrap ? pmL : pm, m);  // p e[p], canonical
-                                const u64 y = canon(shoup_mul_lazy(dv + P - pe, c, cq, P));
-                                rg.x[j] = mont_mul(y, wrap ? fwrap : f[j % NCH], m);
-                            } else {
-                                // p e[p]: with p floor(2^64/p) for the companion the quotient estimate
-                                // loses at most p x / 2^64 < INV_OUT more (x < INV_OUT P, p <= 2^14,
-                                // P < 2^50), so pe < (INV_OUT + 4) P
-                                const u64 pe = shoup_mul_lazy(rg.x[j], (u64)p, (u64)p * mu, P);
-                                check_bound(pe, G::INV_OUT + 4);
-                                const u64 y = shoup_mul_lazy(dv + (G::INV_OUT + 4) * P - pe, c, cq, P);
-                                rg.x[j] = mont_mul(y, wrap ? fwrap : f[j % NCH], m);
-                            }
+                            rg.x[j] = entry(rg.x[j], p, c, cq, wrap ? fwrap : f[j % NCH], wrap ? pmL : pm);
                             st_stream(col + p, rg.x[j]);
                         }
                         f[j % NCH] = chain_step(f[j % NCH], step, stepq);

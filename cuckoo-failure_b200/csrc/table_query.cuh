@@ -11,14 +11,18 @@
 
 namespace cfb {
 
+// Queries per launch: their sizes travel in the kernel parameters (no staging buffer, so launches
+// on several streams never share one).
+constexpr int TQ_MAXJ = 256;
 struct TQParams {
     const u64* primes;  // [B]
     int B, n, F, d, d0, model, J;
-    const int* qn;      // [J], each <= n
-    const int* qM;      // [J], each <= F
     const u64* keep;    // [B][keep_words]
     size_t keep_words;
-    u64* out;           // [B][J]
+    u64* out;           // residue of prime b, query jq at out[b * out_stride + jq]
+    size_t out_stride;
+    int qn[TQ_MAXJ];    // each <= n
+    int qM[TQ_MAXJ];    // each <= F
 };
 
 // One CTA per (prime, query).  Dynamic shared memory: the row sums ps[0..n] and a reduction area.
@@ -87,7 +91,7 @@ __global__ void __launch_bounds__(T) k_table_query(TQParams tp) {
         u64 r = sh(s, fact, nj);
         r = red2(red2(r, 2 * P), P);
         r = sh(r, fact, Mj);
-        tp.out[(size_t)b * tp.J + jq] = red2(red2(r, 2 * P), P);
+        tp.out[(size_t)b * tp.out_stride + jq] = red2(red2(r, 2 * P), P);
     }
 }
 

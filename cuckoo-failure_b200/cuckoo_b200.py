@@ -59,6 +59,16 @@ def lib():
         L.cf_tables_query.restype = ctypes.c_int
         L.cf_tables_free.argtypes = [ctypes.c_void_p]
         L.cf_tables_free.restype = None
+        L.cf_tables_build_async.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.cf_tables_build_async.restype = ctypes.c_int
+        L.cf_tables_ready.argtypes = [ctypes.c_void_p]
+        L.cf_tables_ready.restype = ctypes.c_int
+        L.cf_tables_query_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _intp, _intp, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_void_p]
+        L.cf_tables_query_async.restype = ctypes.c_int
+        L.cf_engine_set_max_ctas.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.cf_engine_set_max_ctas.restype = ctypes.c_int
         L.cf_transform_length.argtypes = [ctypes.c_uint64]
         L.cf_transform_length.restype = ctypes.c_uint64
         L.cf_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
@@ -216,6 +226,14 @@ class Engine:
         """Plan and capture an uneven batch over instances [(n, M, d)] (cf_uneven_create)."""
         return Uneven(self, instances, model, bits, first, count, stride)
 
+    def tables_async(self, primes, nmax, Fmax, d, model=MODEL_SUBSET, stream_ptr=None):
+        """Enqueue the build of resident tables on a stream (cf_tables_build_async); poll ready()."""
+        return Tables(self, primes, nmax, Fmax, d, model, stream_ptr=stream_ptr or 0, wait=False)
+
+    def set_max_ctas(self, n):
+        """At most n primes (CTAs) per launch of this engine's batches (0: no cap)."""
+        self._check(lib().cf_engine_set_max_ctas(self._h, n))
+
     def max_batch(self, nmax, Mmax, J):
         return int(lib().cf_max_batch(self._h, nmax, Mmax, J))
 
@@ -344,14 +362,32 @@ class Tables:
     """Resident tables of a batch of primes (cf_tables_build); query() answers (n, M) with n <= nmax,
     M <= Fmax from them without a rebuild."""
 
-    def __init__(self, engine, primes, nmax, Fmax, d, model=MODEL_SUBSET):
+    def __init__(self, engine, primes, nmax, Fmax, d, model=MODEL_SUBSET, stream_ptr=None, wait=True):
         self.engine, self.nmax, self.Fmax, self.d, self.model = engine, nmax, max(nmax, Fmax), d, model
         self.primes = [int(p) for p in primes]
         p = np.ascontiguousarray(self.primes, dtype=np.uint64)
         h = ctypes.c_void_p()
-        rc = lib().cf_tables_build(engine._h, p.ctypes.data_as(_u64p), len(p), nmax, Fmax, d, model, ctypes.byref(h))
+        if wait:
+            rc = lib().cf_tables_build(engine._h, p.ctypes.data_as(_u64p), len(p), nmax, Fmax, d, model, ctypes.byref(h))
+        else:
+            rc = lib().cf_tables_build_async(engine._h, p.ctypes.data_as(_u64p), len(p), nmax, Fmax, d, model,
+                                             ctypes.c_void_p(stream_ptr), ctypes.byref(h))
         engine._check(rc)
         self._t = h
+
+    def ready(self):
+        """True once the build has finished; raises if its device checks failed."""
+        rc = lib().cf_tables_ready(self._t)
+        if rc < 0:
+            raise EngineError(rc, "resident table build failed")
+        return rc == 1
+
+    def query_async(self, queries, d_out_ptr, stream_ptr=None):
+        """Enqueue the residues of `queries` into device memory [prime][query] on a stream."""
+        qn, qM = _queries(queries)
+        rc = lib().cf_tables_query_async(self.engine._h, self._t, qn.ctypes.data_as(_intp), qM.ctypes.data_as(_intp),
+                                         len(qn), ctypes.c_void_p(d_out_ptr), ctypes.c_void_p(stream_ptr or 0))
+        self.engine._check(rc)
 
     def query(self, queries):
         qn, qM = _queries(queries)

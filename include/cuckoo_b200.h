@@ -130,7 +130,25 @@ int cf_tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, int F
  * qn[j] < qM[j] <= Fmax.  Host buffers; returns when the residues are in `residues`. */
 int cf_tables_query(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, uint64_t* residues);
 int cf_tables_count(const cf_tables* t);
+/* Frees at once; tables built by cf_tables_build_async go back to the stream-ordered pool without
+ * waiting for the device, so the caller must know no query on them is still in flight. */
 void cf_tables_free(cf_tables* t);
+
+/* Serving forms that never wait (the serving loop overlaps builds, queries and plain rebuilds).
+ * cf_tables_build_async: the build of cf_tables_build enqueued on `stream` (memory from the
+ * stream-ordered allocator); cf_tables_ready polls it: 1 when done, 0 while running, CF_ERR_DEVICE
+ * if its device checks failed.  cf_tables_query_async: the residues of J queries into device memory,
+ * d_residues[b * J + j], enqueued on `stream` after whatever the stream already holds (make the
+ * stream wait for the build, or query only ready tables); the query sizes travel in the kernel
+ * parameters, so queries on several streams share no buffer.  No counterpart in the reference. */
+int cf_tables_build_async(cf_engine* e, const uint64_t* primes, int B, int nmax, int Fmax, int d, int model, void* stream,
+                          cf_tables** out);
+int cf_tables_ready(const cf_tables* t);
+int cf_tables_query_async(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, uint64_t* d_residues,
+                          void* stream);
+/* At most n primes (CTAs) per launch for this engine's batches (0: no cap), so a long batch leaves
+ * SMs to work on other streams. */
+int cf_engine_set_max_ctas(cf_engine* e, int n);
 
 /* ---- uneven batches: many instances in one graph of work-queue launches ----
  * Instances k = 0 .. K-1, (n[k], M[k], d[k]) under one model and prime list (bits = 50 or 62):
