@@ -186,44 +186,64 @@ def golden_check(n, M, d, bits=50):
     return out
 
 
-def serving_run(device, seconds, rate=200.0, n_lo=64, n_hi=2048, budget_gb=150.0, plain_sample=16):
-    """Served-query latency: a seeded Poisson stream (rate per second, n log-uniform in [n_lo, n_hi],
-    M = n U[1.5, 4], d in {2, 3, 4}) through serve.py's continuous-batching loop over resident
-    tables built before the clock starts for (n_hi, 4 n_hi, d).  Latencies from arrival to residues
-    ready (GPU) and to exact N_bad (after the host CRT pool).  Beside it the plain form on a sample
-    of the same requests: each rebuilt alone (cf_residues over its primes), to residues ready."""
+def serving_run(device, seconds, rate=200.0, budget_gb=150.0, full_seconds=2.0, drain_s=20.0, plain_nmax=4096):
+    """Served-query latency through serve.py's loop (resident tables, builds on their own stream,
+    queries overlapped on query streams, plain rebuilds on a worker), seeded Poisson streams at
+    `rate` per second with M = n U[1.5, 4] and d in {2, 3, 4}:
+    * the resident range: n log-uniform in [64, 2048] for `seconds`, tables for (2048, 8192, d)
+      built before the clock (they fit the budget for every d);
+    * the full range the workload states, n log-uniform in [64, 16384], for `full_seconds` with
+      the same warm tables; requests above the resident range take the plain path one at a time,
+      least work first (up to n = plain_nmax; a rebuild cannot be interrupted, so larger ones are
+      refused), and the loop stops `drain_s` after the last arrival: what is not answered by then
+      is counted per n bucket.
+    Latencies from arrival to residues ready and to exact N_bad (after the host CRT pool), per n
+    bucket.  Beside them, the plain form: one request of each size class rebuilt alone."""
     import numpy as np
 
     import cuckoo_b200 as cb
     import serve
 
-    stream = serve.poisson_stream(seconds, rate, n_lo, n_hi, seed=20261203)
-    warm = [(n_hi, 4 * n_hi, dd) for dd in (2, 3, 4)]
-    with cb.Engine(device) as eng:
-        t0 = time.perf_counter()
-        kmax = max(cb.need(n, M, dd) for _, n, M, dd in stream)
-        pool = serve.crt_pool(kmax)
-        srv_lat, _, stats = serve.run(stream, eng, budget_gb * 1e9, warm=warm, pool=pool)
-        pool.shutdown()
-        total = time.perf_counter() - t0
-        plain = []
-        for _, n, M, dd in stream[:: max(1, len(stream) // plain_sample)][:plain_sample]:
-            s0 = time.perf_counter()
-            eng.residues(cb.prime_range(0, cb.need(n, M, dd)), n, dd, [(n, M)])
-            plain.append(time.perf_counter() - s0)
-    nb = serve.percentiles(srv_lat)
-    rl = stats["residues_latency"]
-    warm_builds = sum((cb.need(*w, cb.MODEL_SUBSET) + serve.CHUNK - 1) // serve.CHUNK for w in warm)
-    return {"workload": f"Poisson {rate:g} req/s for {seconds:g} s, n log-uniform [{n_lo}, {n_hi}], M/n U[1.5, 4], "
-                        f"d in {{2,3,4}}; tables resident (built before the clock) under a {budget_gb:g} GB budget",
-            "p50_ms": rl.get("p50_ms"), "p99_ms": rl.get("p99_ms"), "latency_to": "residues ready",
-            "nbad_p50_ms": nb.get("p50_ms"), "nbad_p99_ms": nb.get("p99_ms"),
-            "requests": stats["requests"], "rounds": stats["rounds"], "requests_per_s": stats["requests"] / stats["wall_s"],
-            "builds_during_stream": stats["builds"] - warm_builds, "plain_path_requests": stats["plain"],
-            "resident_gb": stats["resident_gb"], "engine_s": stats["engine_s"], "warmup_and_stream_s": total,
-            "plain_rebuild_p50_ms": 1e3 * float(np.median(plain)) if plain else None, "plain_sample": len(plain),
-            "note": "n above ~2048 cannot stay resident for d = 2..4 within the budget (a table at n = 16384 is "
-                    "1.07 GB per prime, 14184 primes at d = 3); such requests take the plain path"}
+    warm = [(2048, 8192, dd) for dd in (2, 3, 4)]
+    out = {}
+    be = serve.GpuBackend(device)
+    try:
+        for key, secs, n_hi, drain in (("resident_range", seconds, 2048, None), ("full_range", full_seconds, 16384, drain_s)):
+            stream = serve.poisson_stream(secs, rate, 64, n_hi, seed=20261203)
+            kmax = max(cb.need(n, M, dd) for _, n, M, dd in stream)
+            pool = serve.crt_pool(kmax)
+            lat, _, st = serve.run(stream, be, budget_gb * 1e9, warm=warm, pool=pool, drain_s=drain,
+                                   plain_nmax=plain_nmax if drain is not None else None)
+            pool.shutdown()
+            rl = st["residues_latency"]
+            nb = serve.percentiles(lat)
+            out[key] = {
+                "workload": f"Poisson {rate:g} req/s for {secs:g} s, n log-uniform [64, {n_hi}], M/n U[1.5, 4], "
+                            f"d in {{2,3,4}}; {budget_gb:g} GB table budget; tables for n <= 2048 built before the clock",
+                "p50_ms": rl.get("p50_ms"), "p99_ms": rl.get("p99_ms"), "latency_to": "residues ready",
+                "nbad_p50_ms": nb.get("p50_ms"), "nbad_p99_ms": nb.get("p99_ms"),
+                "buckets_nbad": serve.bucketed(stream, lat),
+                "requests": st["requests"], "answered": st["answered"], "plain_path_requests": st["plain"],
+                "refused_plain_above_n": plain_nmax if drain is not None else None, "refused": st["refused"],
+                "builds_during_stream": st["builds"], "query_launches": st["query_launches"],
+                "requests_per_s": st["answered"] / st["wall_s"], "resident_gb": st["resident_gb"], "wall_s": st["wall_s"]}
+        with cb.Engine(device) as eng:  # the plain form: one request rebuilt alone, per size class
+            plain = {}
+            for n in (256, 1024, 4096):
+                M, dd = 3 * n, 3
+                ps = cb.prime_range(0, cb.need(n, M, dd))
+                eng.residues(ps[:2], n, dd, [(n, M)])
+                t0 = time.perf_counter()
+                eng.residues(ps, n, dd, [(n, M)])
+                plain[f"n={n},M={M},d={dd}"] = {"primes": len(ps), "ms": 1e3 * (time.perf_counter() - t0)}
+        out["plain_rebuild"] = plain
+        out["note"] = ("a table at n = 16384 is 1.07 GB per prime and a d = 3 request there needs 14184 primes (15 TB): "
+                       "n above ~2048 cannot stay resident for d = 2..4 within the budget, and one such request alone "
+                       "takes the plain path's full-GPU time (about need / rate: minutes at n = 16384); the full-range "
+                       "stream offers far more plain work than the GPU can do, so its upper buckets stay unanswered")
+    finally:
+        be.close()
+    return out
 
 
 def timed_replays(launch, stream, reps):
@@ -244,43 +264,91 @@ def timed_replays(launch, stream, reps):
 def uneven_run(eng, stride, per_instance_count=32, seed=None):
     """The uneven-batch workload (512 instances: n log-uniform in [256, 16384], M = n U{2, 3, 4},
     d in {2, 3, 4}, seed-fixed), every instance modulo its own need(n, M, d) primes, on the prime
-    indices that are multiples of `stride` (a sample whose tables follow the whole run's mix).
-    Timed as one graph of work-queue launches, beside the plain form: each instance alone, one
-    cf_residues call (a launch per chunk of primes) per instance, on the first per_instance_count
-    instances and the same prime indices."""
-    import numpy as np
-    import torch
-
+    indices that are multiples of `stride` (a sample whose tables follow the whole run's mix),
+    as one graph of work-queue launches.  Beside it the plain form, each instance alone (one
+    cf_residues call, a launch per chunk of primes, per instance), measured like for like against
+    the graph on the first per_instance_count instances and the same primes; and a work model of
+    the whole run (sum over tables of (n - 1) L (lg L + 1), in tables of n = 16384) for both forms."""
     import cuckoo_b200 as cb
     import uneven
 
     insts = uneven.instances(512, seed=seed or uneven.CONFIG4_SEED)
     needs = [cb.need(n, M, d) for n, M, d in insts]
     planned = [len(range(0, k, stride)) for k in needs]
-    stream = torch.cuda.Stream()
-    with eng.uneven(insts, stride=stride) as u:
-        ms = timed_replays(u.launch, stream, 1)
-        res = u.results(stream.cuda_stream)
-        tables, launches = u.tables(), u.launches()
-    full_tables = len(cb.uneven_describe(insts))
+
+    def graph_time(instances):
+        import torch
+
+        stream = torch.cuda.Stream()
+        with eng.uneven(instances, stride=stride) as u:
+            ms = timed_replays(u.launch, stream, 1)
+            return ms, u.results(stream.cuda_stream), u.tables(), u.launches()
+
+    ms, res, tables, launches = graph_time(insts)
     sub = insts[:per_instance_count]
+    sub_ms, sub_res, sub_tables, _ = graph_time(sub)
     t0 = time.perf_counter()
     alone = uneven.per_instance(eng, sub, cb.prime_range, cb.need, stride=stride)
     plain_s = time.perf_counter() - t0
-    for k in range(len(sub)):  # the same residues both ways
-        assert [int(x) for x in res[k][::stride]] == alone[k][::stride], f"uneven instance {k} differs"
-    sub_residues = sum(planned[:per_instance_count])
-    sub_share = sub_residues / max(1, sum(planned))
+    for k in range(len(sub)):  # the same residues every way
+        assert [int(x) for x in res[k][::stride]] == [int(x) for x in sub_res[k][::stride]] == alone[k][::stride], \
+            f"uneven instance {k} differs"
+
+    def cost(n):
+        L = cb.transform_length(n)
+        return (n - 1) * L * L.bit_length()
+
+    full = cb.uneven_describe(insts)
+    c16 = cost(16384)
+    queue_equiv = sum(cost(t[3]) for t in full) / c16
+    plain_equiv = sum(k * cost(n) for (n, _, _), k in zip(insts, needs)) / c16
     return {"workload": "512 instances, n log-uniform [256, 16384], M = n U{2,3,4}, d U{2,3,4}, "
                         f"seed {uneven.CONFIG4_SEED}; prime indices i = 0 mod {stride} of each instance's need",
-            "tables": tables, "tables_full_run": full_tables, "launches_per_graph": launches,
-            "instance_residues": sum(planned), "ms": ms,
-            "instance_residues_per_s": sum(planned) / (ms * 1e-3), "tables_per_s": tables / (ms * 1e-3),
-            "full_run_s_est": full_tables / (tables / (ms * 1e-3)),
-            "per_instance_form": {"instances": per_instance_count, "instance_residues": sub_residues,
-                                  "s": plain_s, "instance_residues_per_s": sub_residues / plain_s,
-                                  "full_run_s_est": plain_s / sub_share,
-                                  "what": "each instance alone: one cf_residues call over its planned primes, its own n"}}
+            "graph": {"tables": tables, "launches_per_graph": launches, "ms": ms, "tables_per_s": tables / (ms * 1e-3),
+                      "instance_residues": sum(planned), "instance_residues_per_s": sum(planned) / (ms * 1e-3),
+                      "tables_full_run": len(full), "full_run_s_est": len(full) / (tables / (ms * 1e-3))},
+            "like_for_like": {"instances": per_instance_count, "instance_residues": sum(planned[:per_instance_count]),
+                              "graph_ms": sub_ms, "graph_tables": sub_tables, "per_instance_s": plain_s,
+                              "speedup": plain_s / (sub_ms * 1e-3),
+                              "what": "the first instances, same primes: one graph against one cf_residues call per instance"},
+            "work_model": {"graph_tables_of_n16384": queue_equiv, "per_instance_tables_of_n16384": plain_equiv,
+                           "ratio": plain_equiv / queue_equiv,
+                           "what": "whole run: one table per (d, prime) at its largest n, against one per (instance, prime)"}}
+
+
+def config2_run(device, n=4096, M=8192, d=3, waves=4, reps=3):
+    """The batch-scale configuration (n = 4096, M = 8192, d = 3): the engine's geometries for
+    transform length 2^12 timed by the autotuner on `waves` x #SMs primes, then the chosen and the
+    default geometry each timed as one graph-captured launch of that batch, the residues of primes
+    0..3 checked against the reference's."""
+    import numpy as np
+    import torch
+
+    import cuckoo_b200 as cb
+
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    B = waves * sms
+    out = {"workload": f"n={n}, M={M}, d={d}, {B} primes per launch"}
+    stream = torch.cuda.Stream()
+    with cb.Engine(device) as eng:
+        rec = eng.autotune(n, M, d, B)
+        out["autotune"] = rec
+        primes = cb.prime_range(0, B)
+        d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
+        d_out = torch.empty(B, dtype=torch.int64, device="cuda")
+        gold = golden_check(n, M, d)
+        for label, k in (("default", 0), ("tuned", rec["chosen"])):
+            eng.tune_set(rec["lg"], k)
+            g = eng.batch_graph(d_primes.data_ptr(), B, n, d, [(n, M)], d_out.data_ptr())
+            ms = timed_replays(g.launch, stream, reps)
+            g.status(stream.cuda_stream)
+            g.close()
+            got = d_out.cpu().numpy().view(np.uint64)
+            for i, r in gold.items():
+                assert int(got[i]) == r, f"config 2 ({label}): residue mismatch at prime {i}"
+            out[label] = {"geometry": rec["variants"][k], "value": B / (ms * 1e-3), "unit": UNIT, "ms_per_launch": ms,
+                          "frac_top": B * algorithmic_mm(n) * K_OPS_PER_MM / (ms * 1e-3) / 1e12}
+    return out
 
 
 def sweep_run(eng, n, M, B, reps=2):
@@ -329,9 +397,12 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the served-query latency run")
     ap.add_argument("--no-plain-form", action="store_true", help="skip the one-prime-per-launch timing")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-full-seconds", type=float, default=2.0,
+                    help="length of the full-range (n up to 16384) serving stream")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch (512 instances) run")
     ap.add_argument("--uneven-stride", type=int, default=97)
     ap.add_argument("--no-sweep", action="store_true", help="skip d = 2, 4 and the replacement model")
+    ap.add_argument("--no-config2", action="store_true", help="skip the n = 4096 (autotuned) run")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="--impl reference: skip the reference's CUDA build (timed beside its host build)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
@@ -484,6 +555,11 @@ def main():
             sweep = sweep_run(eng2, n, M, B)
         for v in sweep.values():
             v["frac"] = v["frac"] / peak if peak else None
+    cfg2 = None
+    if rank == 0 and world == 1 and not a.no_config2:
+        cfg2 = config2_run(local)
+        for k in ("default", "tuned"):
+            cfg2[k]["frac"] = cfg2[k].pop("frac_top") / peak if peak else None
     unev = None
     if rank == 0 and world == 1 and not a.no_uneven:
         with cb.Engine(local) as eng2:
@@ -493,7 +569,7 @@ def main():
         cpu = cpu_baseline(n, M, d)
     serving = None
     if rank == 0 and world == 1 and not a.no_serving:
-        serving = serving_run(local, a.serve_seconds)
+        serving = serving_run(local, a.serve_seconds, full_seconds=a.serve_full_seconds)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -507,7 +583,7 @@ def main():
                          "model": f"{K_OPS_PER_MM} INT32 multiply ops per modular multiplication, "
                                   f"{algorithmic_mm(n):.3e} multiplications per prime-residue; peak measured live"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-            "plain_form": plain, "config3_sweep": sweep, "uneven": unev, "serving": serving}))
+            "plain_form": plain, "config2": cfg2, "config3_sweep": sweep, "uneven": unev, "serving": serving}))
     if dist:
         dist.destroy_process_group()
     return 0

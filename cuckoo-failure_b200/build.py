@@ -31,7 +31,8 @@ NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xpt
 # 320 bytes.  The L = 2^10 kernel is compiled for 16 CTAs per SM (MinBlocks in kernel_lg.cuh), also
 # 128 registers: -O1 keeps it to a 208-byte frame where the default level spills 1.4 KB.  The other
 # kernels have up to 255 registers and spill at neither level.
-UNIT_FLAGS = {"k_lg14.cu": ["-Xptxas", "-O1"], "k_lg10.cu": ["-Xptxas", "-O1"]}
+UNIT_FLAGS = {"k_lg14.cu": ["-Xptxas", "-O1"], "k_lg10.cu": ["-Xptxas", "-O1"],
+              "k_lg14_tune.cu": ["-Xptxas", "-O1"], "k_lg10_tune.cu": ["-Xptxas", "-O1"]}
 
 
 def newest_dep():

@@ -47,18 +47,51 @@ KInfo kernel_for(int lg, bool wide) {
         default: return KInfo{nullptr, 0, 0, 0};
     }
 }
+int cf_kvariants_lg10(KInfo* out, int cap);
+int cf_kvariants_lg11(KInfo* out, int cap);
+int cf_kvariants_lg12(KInfo* out, int cap);
+int cf_kvariants_lg13(KInfo* out, int cap);
+int cf_kvariants_lg14(KInfo* out, int cap);
+// The geometries compiled for transform length 2^lg (50-bit kernel), the default first.
+static int variants_for(int lg, KInfo* v, int cap) {
+    switch (lg) {
+        case 10: return cf_kvariants_lg10(v, cap);
+        case 11: return cf_kvariants_lg11(v, cap);
+        case 12: return cf_kvariants_lg12(v, cap);
+        case 13: return cf_kvariants_lg13(v, cap);
+        case 14: return cf_kvariants_lg14(v, cap);
+        default:
+            if (cap > 0) v[0] = kernel_for(lg);
+            return kernel_for(lg).fn ? 1 : 0;
+    }
+}
+constexpr int MAX_VARIANTS = 8;
+// The kernel an engine runs: for primes below 2^50 the geometry it was tuned to, else the default.
+static KInfo kernel_of(const cf_engine* e, int lg, bool wide) {
+    if (!wide && e && lg >= 0 && lg <= MAX_LG && e->tuned[lg] > 0) {
+        KInfo v[MAX_VARIANTS];
+        if (e->tuned[lg] < variants_for(lg, v, MAX_VARIANTS)) return v[e->tuned[lg]];
+    }
+    return kernel_for(lg, wide);
+}
+
 struct Plan {
-    int lg, F, d0;
+    int lg, F, d0, nmax, J;
     bool wide = false;  // some prime is 2^50 or above: the kernels for primes below 2^62
+    KInfo ki;           // the kernel that runs the batch
     Layout lay;
     size_t ws_words;
 };
-// warps per CTA of the kernel for transform length 2^lg (query partial sums are kept per warp)
-static int warps_for(int lg) {
-    const KInfo ki = kernel_for(lg);
-    return ki.threads >= 32 ? ki.threads / 32 : 1;
+// The kernel this engine runs for the plan and the workspace layout its geometry needs (the
+// pass-0 twiddle tables follow the entries per thread); again whenever wide or F changes.
+static int finalize(cf_engine* e, Plan& pl) {
+    pl.ki = kernel_of(e, pl.lg, pl.wide);
+    if (!pl.ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
+    const int nw = pl.ki.threads >= 32 ? pl.ki.threads / 32 : 1;
+    pl.lay = make_layout(pl.nmax, pl.F, 1 << pl.lg, pl.J, nw, pl.ki.r);
+    pl.ws_words = pl.lay.total;
+    return CF_OK;
 }
-static int r_for(int lg) { return kernel_for(lg).r; }
 
 static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const int* qM, int J, Plan& pl) {
     if (nmax < 1 || d < 1 || (model != CF_MODEL_SUBSET && model != CF_MODEL_REPLACEMENT) || J < 0)
@@ -78,9 +111,10 @@ static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const i
     pl.lg = lg;
     pl.F = F;
     pl.d0 = model == CF_MODEL_SUBSET ? d : 1;
-    pl.lay = make_layout(nmax, F, (int)L, J, warps_for(lg), r_for(lg));
-    pl.ws_words = pl.lay.total;
-    return CF_OK;
+    pl.nmax = nmax;
+    pl.J = J;
+    pl.wide = false;
+    return finalize(e, pl);
 }
 
 static int check_primes(cf_engine* e, const u64* primes, int B, Plan& pl) {
@@ -92,7 +126,7 @@ static int check_primes(cf_engine* e, const u64* primes, int B, Plan& pl) {
             return fail(e, CF_ERR_ARG, "prime " + std::to_string(p) + " is not an odd prime < 2^62 above max(n, M) with L | p-1");
         if (p >= (1ull << 50)) pl.wide = true;
     }
-    return CF_OK;
+    return finalize(e, pl);
 }
 
 static int ensure_ws(cf_engine* e, size_t bytes) {
@@ -144,7 +178,7 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
                         u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0, bool fixed_ws = false,
                         int* err = nullptr) {
     if (!err) err = e->d_err;
-    const KInfo ki = kernel_for(pl.lg, pl.wide);
+    const KInfo ki = pl.ki;
     if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     const size_t smem = ki.smem_for(J);
     int rc0 = check_smem(e, smem, J);
@@ -266,7 +300,8 @@ uint64_t cf_workspace_bytes(int nmax, int Mmax, int J) {
     int lg = 0;
     while ((1ull << lg) < L) ++lg;
     if (lg > MAX_LG) return 0;
-    return 8 * make_layout(nmax, F, (int)L, J, warps_for(lg), r_for(lg)).total;
+    const KInfo ki = kernel_for(lg);
+    return 8 * make_layout(nmax, F, (int)L, J, ki.threads >= 32 ? ki.threads / 32 : 1, ki.r).total;
 }
 
 // ---- resident tables (serving) ----
@@ -303,9 +338,7 @@ static int tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, i
     int rc = plan(e, nmax, d, model, nullptr, nullptr, 0, pl);
     if (rc) return rc;
     pl.F = std::max(pl.F, Fmax);  // the largest M later queries may use
-    pl.lay = make_layout(nmax, pl.F, 1 << pl.lg, 0, warps_for(pl.lg), r_for(pl.lg));
-    pl.ws_words = pl.lay.total;
-    rc = check_primes(e, primes, B, pl);
+    rc = check_primes(e, primes, B, pl);  // and the layout for that F
     if (rc) return rc;
     if (pl.wide) return fail(e, CF_ERR_UNSUPPORTED, "resident tables hold primes below 2^50");
     CF_CUDA(cudaSetDevice(e->device), "set device");
@@ -475,6 +508,8 @@ int cf_residues_async(cf_engine* e, const uint64_t* d_primes, int B, int nmax, i
     if (rc) return rc;
     if (B == 0) return CF_OK;
     pl.wide = e->prime_bits > 50;
+    rc = finalize(e, pl);
+    if (rc) return rc;
     CF_CUDA(cudaSetDevice(e->device), "set device");
     cudaStream_t s = (cudaStream_t)stream;  // NULL is the CUDA default stream
     rc = ensure_queries(e, qn, qM, J, s);
@@ -554,6 +589,8 @@ int cf_batch_graph_create(cf_engine* e, const uint64_t* d_primes, int B, int nma
     int rc = plan(e, nmax, d, model, qn, qM, J, pl);
     if (rc) return rc;
     pl.wide = e->prime_bits > 50;
+    rc = finalize(e, pl);
+    if (rc) return rc;
     CF_CUDA(cudaSetDevice(e->device), "set device");
     cf_batch_graph* g = new cf_batch_graph();
     g->device = e->device;
@@ -573,8 +610,6 @@ int cf_batch_graph_create(cf_engine* e, const uint64_t* d_primes, int B, int nma
         if (fitb < 1) return fail(e, CF_ERR_NOMEM, "not enough device memory for one prime");
         r = ensure_ws(e, (size_t)std::min<long>(B, fitb) * per_prime);
         if (r) return r;
-        const KInfo ki = kernel_for(pl.lg, pl.wide);
-        if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
         CF_CUDA(cudaStreamSynchronize(cs), "query upload");
         CF_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
         r = launch_batch(e, d_primes, B, nmax, d, model, J, pl, d_residues, cs, nullptr, 0, true);
@@ -617,5 +652,74 @@ int cf_batch_graph_status(cf_batch_graph* g, void* stream) {
 }
 
 long cf_batch_graph_launches(const cf_batch_graph* g) { return g ? g->launches : 0; }
+
+// ---- autotuning of the kernel geometry ----
+
+int cf_tune_variants(int lg, int* log2_entries, int* threads, int* ctas_per_sm, int cap) {
+    if (lg < 0 || lg > MAX_LG || cap < 0) return -1;
+    KInfo v[MAX_VARIANTS];
+    const int k = variants_for(lg, v, MAX_VARIANTS);
+    for (int i = 0; i < k && i < cap; ++i) {
+        if (log2_entries) log2_entries[i] = v[i].r;
+        if (threads) threads[i] = v[i].threads;
+        if (ctas_per_sm) ctas_per_sm[i] = v[i].mb;
+    }
+    return k;
+}
+
+int cf_tune_set(cf_engine* e, int lg, int variant) {
+    if (!e || lg < 0 || lg > MAX_LG || variant < 0) return CF_ERR_ARG;
+    KInfo v[MAX_VARIANTS];
+    if (variant >= variants_for(lg, v, MAX_VARIANTS)) return CF_ERR_ARG;
+    e->tuned[lg] = variant;
+    return CF_OK;
+}
+
+int cf_tune_get(const cf_engine* e, int lg) { return e && lg >= 0 && lg <= MAX_LG ? e->tuned[lg] : -1; }
+
+int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, int cap, int* chosen) {
+    if (!e || B < 1 || nmax < 1) return CF_ERR_ARG;
+    e->err.clear();
+    const u64 L = cfh::transform_length((u64)nmax);
+    int lg = 0;
+    while ((1ull << lg) < L) ++lg;
+    if (lg > MAX_LG) return fail(e, CF_ERR_UNSUPPORTED, "transform length above 2^14");
+    KInfo v[MAX_VARIANTS];
+    const int k = variants_for(lg, v, MAX_VARIANTS);
+    const std::vector<u64> primes = cfh::prime_range(0, B);
+    const int qn[1] = {nmax}, qM[1] = {std::max(Mmax, nmax + 1)};
+    std::vector<u64> first_out, out((size_t)B);
+    const int saved = e->tuned[lg];
+    int best = 0;
+    double best_rate = -1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CF_CUDA(cudaSetDevice(e->device), "set device");
+    CF_CUDA(cudaEventCreate(&e0), "event");
+    CF_CUDA(cudaEventCreate(&e1), "event");
+    int rc = CF_OK;
+    for (int i = 0; i < k && rc == CF_OK; ++i) {
+        e->tuned[lg] = i;
+        float ms = 0;
+        for (int rep = 0; rep < 2 && rc == CF_OK; ++rep) {  // a warm-up launch, then the timed one
+            if (cudaEventRecord(e0, e->stream) != cudaSuccess) rc = fail(e, CF_ERR_CUDA, "event");
+            if (rc == CF_OK) rc = cf_residues(e, primes.data(), B, nmax, d, CF_MODEL_SUBSET, qn, qM, 1, out.data());
+            if (rc == CF_OK && (cudaEventRecord(e1, e->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                rc = fail(e, CF_ERR_CUDA, "timing");
+        }
+        if (rc) break;
+        if (i == 0) first_out = out;
+        else if (out != first_out)  // every geometry computes the same residues
+            rc = fail(e, CF_ERR_DEVICE, "geometry " + std::to_string(i) + " disagrees with the default");
+        const double rate = B / (ms * 1e-3);
+        if (rates && i < cap) rates[i] = rate;
+        if (rate > best_rate) best_rate = rate, best = i;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    e->tuned[lg] = rc == CF_OK ? best : saved;
+    if (chosen) *chosen = e->tuned[lg];
+    return rc;
+}
 
 }  // extern "C"

@@ -57,6 +57,7 @@ struct cf_engine {
     long launches = 0;
     int prime_bits = 50;  // for cf_residues_async, whose primes are not read on the host
     int max_ctas = 0;     // CTAs (primes) per launch at most, 0 = no cap
+    int tuned[MAX_LG + 1] = {};  // geometry (index into the compiled variants) per transform length
     std::string err;
 };
 

@@ -1,0 +1,15 @@
+// Autotuning candidates for transform length 2^12: the default geometry (k_lg12.cu) first,
+// then other (entries per thread, CTAs per SM) pairs of the 50-bit kernel.
+#include "kernel_lg.cuh"
+
+cfb::KInfo cf_kinfo_lg12();
+int cf_kvariants_lg12(cfb::KInfo* out, int cap) {
+    const cfb::KInfo v[] = {
+        cf_kinfo_lg12(),
+        cfb::kinfo_geo<12, 4, 2>(),
+        cfb::kinfo_geo<12, 3, 2>(),
+        cfb::kinfo_geo<12, 5, 1>()};
+    const int k = (int)(sizeof(v) / sizeof(v[0]));
+    for (int i = 0; i < k && i < cap; ++i) out[i] = v[i];
+    return k;
+}

@@ -97,8 +97,9 @@ template <int LG>
 struct MinBlocks {
     static constexpr int v = LG == 10 ? 16 : 1;
 };
-template <int LG, int R, bool W>
-__global__ void __launch_bounds__(Geo<LG, R>::T, MinBlocks<LG>::v) k_suffix(KParams kp) {
+// MB: resident CTAs per SM the variant is compiled for (its register cap).
+template <int LG, int R, bool W, int MB = MinBlocks<LG>::v>
+__global__ void __launch_bounds__(Geo<LG, R>::T, MB) k_suffix(KParams kp) {
     typedef Geo<LG, R> G;
     extern __shared__ __align__(16) u64 smem[];
     DevExec<G> ex;
@@ -173,14 +174,22 @@ struct KInfo {
     int threads;
     size_t smem;  // fixed dynamic shared memory; a launch with J queries adds 8 J (threads / 32)
     int r;        // log2 of the entries per thread
-    qfn_t qfn;    // the work-queue form
+    qfn_t qfn;    // the work-queue form (the default geometry only)
+    int mb;       // resident CTAs per SM the kernel is compiled for
     size_t smem_for(int J) const { return smem + (size_t)8 * J * (threads >= 32 ? threads / 32 : 1); }
 };
 // W selects the kernel for primes below 2^62 (otherwise below 2^50).
 template <int LG, bool W = false>
 inline KInfo kinfo() {
     typedef Geo<LG, RFor<LG>::R> G;
-    return KInfo{&k_suffix<LG, RFor<LG>::R, W>, G::T, Smem<G>::BYTES, RFor<LG>::R, &k_suffix_queue<LG, RFor<LG>::R, W>};
+    return KInfo{&k_suffix<LG, RFor<LG>::R, W>, G::T, Smem<G>::BYTES, RFor<LG>::R, &k_suffix_queue<LG, RFor<LG>::R, W>,
+                 MinBlocks<LG>::v};
+}
+// Another geometry of the 50-bit kernel (autotuning candidates): 2^R entries per thread, MB CTAs per SM.
+template <int LG, int R, int MB>
+inline KInfo kinfo_geo() {
+    typedef Geo<LG, R> G;
+    return KInfo{&k_suffix<LG, R, false, MB>, G::T, Smem<G>::BYTES, R, nullptr, MB};
 }
 
 }  // namespace cfb

@@ -69,6 +69,15 @@ def lib():
         L.cf_tables_query_async.restype = ctypes.c_int
         L.cf_engine_set_max_ctas.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.cf_engine_set_max_ctas.restype = ctypes.c_int
+        L.cf_tune_variants.argtypes = [ctypes.c_int, _intp, _intp, _intp, ctypes.c_int]
+        L.cf_tune_variants.restype = ctypes.c_int
+        L.cf_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.c_int, _intp]
+        L.cf_autotune.restype = ctypes.c_int
+        L.cf_tune_set.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.cf_tune_set.restype = ctypes.c_int
+        L.cf_tune_get.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.cf_tune_get.restype = ctypes.c_int
         L.cf_transform_length.argtypes = [ctypes.c_uint64]
         L.cf_transform_length.restype = ctypes.c_uint64
         L.cf_engine_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
@@ -155,6 +164,14 @@ def lib_primes(n, M, d, model=MODEL_SUBSET):
     return [int(x) for x in out]
 
 
+def tune_variants(lg):
+    """The compiled geometries for transform length 2^lg, the default first:
+    [{"entries_per_thread": 2^r, "threads": T, "ctas_per_sm": k}]."""
+    r, t, m = (np.zeros(8, dtype=np.int32) for _ in range(3))
+    k = int(lib().cf_tune_variants(lg, r.ctypes.data_as(_intp), t.ctypes.data_as(_intp), m.ctypes.data_as(_intp), 8))
+    return [{"entries_per_thread": 1 << int(r[i]), "threads": int(t[i]), "ctas_per_sm": int(m[i])} for i in range(k)]
+
+
 def workspace_bytes(nmax, Mmax, J):
     return int(lib().cf_workspace_bytes(nmax, Mmax, J))
 
@@ -229,6 +246,22 @@ class Engine:
     def tables_async(self, primes, nmax, Fmax, d, model=MODEL_SUBSET, stream_ptr=None):
         """Enqueue the build of resident tables on a stream (cf_tables_build_async); poll ready()."""
         return Tables(self, primes, nmax, Fmax, d, model, stream_ptr=stream_ptr or 0, wait=False)
+
+    def autotune(self, nmax, Mmax, d, B):
+        """Time every compiled geometry for nmax's transform length on B primes (cf_autotune) and
+        keep the fastest: returns {"lg", "chosen", "rates" (primes/s per geometry), "variants"}."""
+        lg = transform_length(nmax).bit_length() - 1
+        rates = (ctypes.c_double * 8)()
+        chosen = ctypes.c_int(0)
+        self._check(lib().cf_autotune(self._h, nmax, Mmax, d, B, rates, 8, ctypes.byref(chosen)))
+        vs = tune_variants(lg)
+        return {"lg": lg, "chosen": chosen.value, "rates": [rates[i] for i in range(len(vs))], "variants": vs}
+
+    def tune_set(self, lg, variant):
+        self._check(lib().cf_tune_set(self._h, lg, variant))
+
+    def tune_get(self, lg):
+        return int(lib().cf_tune_get(self._h, lg))
 
     def set_max_ctas(self, n):
         """At most n primes (CTAs) per launch of this engine's batches (0: no cap)."""

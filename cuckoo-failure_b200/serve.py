@@ -1,5 +1,5 @@
 #!/usr/bin/env python3
-"""Continuous-batching query server over resident suffix tables.
+"""Continuous-batching query server over resident suffix tables, with its device work overlapped.
 
 A request nbad(n, M, d) is answered as the reference answers it: N_bad modulo the first
 need(n, M, d) primes of the fixed list (fast/cuckoo_fast.cu:403-459), recombined by CRT
@@ -10,22 +10,31 @@ with n' <= n, M' <= F in O(n'^2) per prime.  A chunk is built, or rebuilt larger
 request needs more than it holds; chunks are admitted under an HBM budget and evicted least
 recently used.
 
-Each round of the loop takes every request that has arrived (continuous batching: requests
-arriving while the GPU works join the next round), builds the chunks the round is missing, and
-answers all of the round's requests per chunk with one query launch.  A request whose tables
-cannot be resident within the budget is computed the plain way (cf_residues, no residency) in
-its round.  The residues of a served request cover whole chunks (the primes beyond its need
-change nothing: N_bad is below the product of its own primes), so every CRT is over a prefix of
-the list whose length is a multiple of the chunk, and a pool of host processes (crt.PrefixCRT,
-constants cached at start) recombines them while the GPU serves the next round.  Two latencies
-are kept per request, from its arrival: residues ready, and N_bad ready.
+Nothing in the loop waits for the device:
+* every pass of the loop admits the requests that have arrived (continuous batching), and for
+  each chunk that is ready sends the waiting requests' queries as one stream-ordered launch on one
+  of a few query streams; results come back through pinned host buffers whose events the loop polls;
+* a chunk's build runs on its own stream (cf_tables_build_async) while queries on the ready
+  chunks go on; requests that need a chunk still being built wait for it in the queue;
+* a request whose tables cannot be resident within the budget takes the plain path: it is rebuilt
+  for that request alone (cf_residues) on a worker thread with its own engine, shortest first, its
+  launches capped to part of the SMs so resident queries keep running beside it.
+The residues of a served request cover whole chunks (the primes beyond its need change nothing:
+N_bad is below the product of its own primes), so every CRT is over a prefix of the list whose
+length is a multiple of the chunk, and a pool of host processes (crt.PrefixCRT, constants cached
+at start) recombines them.  Two latencies are kept per request, from its arrival: residues ready,
+and N_bad ready.
 
     python cuckoo-failure_b200/serve.py [--seconds 10] [--rate 200] [--nmax 2048] [--budget-gb 150] [--seed 1]
 """
 import argparse
+import concurrent.futures as cf
+import heapq
+import itertools
 import math
 import os
 import sys
+import threading
 import time
 from collections import OrderedDict
 
@@ -66,85 +75,295 @@ def grow(x, lo=64):
     return 1 << (k + 1)
 
 
+# ---------------------------------------------------------------------------------------------
+# Device side
+# ---------------------------------------------------------------------------------------------
+class GpuBackend:
+    """The device side of the server on one GPU: resident tables built on a build stream, queries
+    enqueued on query streams into device buffers and copied to pinned host memory, and plain
+    rebuilds on a worker thread with its own engine whose launches take at most plain_ctas SMs."""
+
+    def __init__(self, device=0, query_streams=2, plain_ctas=96):
+        import torch
+
+        self.torch = torch
+        self.device = device
+        torch.cuda.set_device(device)
+        self.eng = cb.Engine(device)
+        self.build_stream = torch.cuda.Stream(device)
+        self.qstreams = [torch.cuda.Stream(device) for _ in range(query_streams)]
+        self._rr = itertools.cycle(range(query_streams))
+        self.plain_ctas = plain_ctas
+        self._plain_local = threading.local()
+        self.plain_pool = cf.ThreadPoolExecutor(1)
+
+    def build(self, primes, nmax, Fmax, d, model):
+        return self.eng.tables_async(primes, nmax, Fmax, d, model, self.build_stream.cuda_stream)
+
+    @staticmethod
+    def ready(tab):
+        return tab.ready()
+
+    def query(self, tab, queries):
+        torch = self.torch
+        qs = self.qstreams[next(self._rr)]
+        B, J = len(tab.primes), len(queries)
+        d_out = torch.empty(B * J, dtype=torch.int64, device=f"cuda:{self.device}")
+        host = torch.empty(B * J, dtype=torch.int64, pin_memory=True)
+        qs.wait_stream(torch.cuda.current_stream(self.device))  # d_out's allocation
+        tab.query_async(queries, d_out.data_ptr(), qs.cuda_stream)
+        with torch.cuda.stream(qs):
+            host.copy_(d_out, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(qs)
+        return _GpuTicket(ev, host, d_out, B, J)
+
+    def _plain_engine(self):
+        e = getattr(self._plain_local, "eng", None)
+        if e is None:
+            self.torch.cuda.set_device(self.device)
+            e = cb.Engine(self.device)
+            e.set_max_ctas(self.plain_ctas)
+            self._plain_local.eng = e
+        return e
+
+    def plain(self, primes, n, M, d, model):
+        """Future of the residues [prime] of (n, M) rebuilt alone, on the worker."""
+        return self.plain_pool.submit(lambda: self._plain_engine().residues(primes, n, d, [(n, M)], model=model)[:, 0])
+
+    @staticmethod
+    def free(tab):
+        tab.close()
+
+    def close(self):
+        self.plain_pool.shutdown(wait=True)
+        self.eng.close()
+
+
+class _GpuTicket:
+    def __init__(self, ev, host, d_out, B, J):
+        self.ev, self.host, self.d_out, self.B, self.J = ev, host, d_out, B, J
+
+    def done(self):
+        return self.ev.query()
+
+    def result(self):
+        self.ev.synchronize()
+        self.d_out = None
+        return self.host.numpy().view(np.uint64).reshape(self.B, self.J)
+
+
+# ---------------------------------------------------------------------------------------------
+# The scheduling loop
+# ---------------------------------------------------------------------------------------------
+class _Chunk:
+    def __init__(self, key, tab, nmax, Fmax, nbytes):
+        self.key, self.tab, self.nmax, self.Fmax, self.bytes = key, tab, nmax, Fmax, nbytes
+        self.ready = False
+        self.inflight = 0  # query launches not yet returned
+
+    def covers(self, n, M):
+        return self.nmax >= n and self.Fmax >= M
+
+
+class _Req:
+    __slots__ = ("rid", "n", "M", "d", "chunks", "got", "plain", "sent")
+
+    def __init__(self, rid, n, M, d, nchunks):
+        self.rid, self.n, self.M, self.d = rid, n, M, d
+        self.chunks = list(range(nchunks))
+        self.got = {}  # chunk -> residues of its primes
+        self.sent = set()  # chunks whose query is in flight
+        self.plain = False
+
+
 class Server:
-    def __init__(self, engine, budget_bytes, model=cb.MODEL_SUBSET, n_cap=16384, chunk=CHUNK):
-        self.eng, self.budget, self.model, self.n_cap, self.chunk = engine, budget_bytes, model, n_cap, chunk
-        self.chunks = OrderedDict()  # (d, chunk index) -> Tables, in LRU order
+    """Request scheduling over a backend (GpuBackend, or a stand-in in tests).
+
+    submit() queues a request; pump() runs one pass of the loop and returns the requests whose
+    residues are complete as [(rid, residues)], residues covering at least need(n, M, d) primes."""
+
+    def __init__(self, backend, budget_bytes, model=cb.MODEL_SUBSET, n_cap=16384, chunk=CHUNK, bytes_fn=None,
+                 plain_nmax=None):
+        self.be, self.budget, self.model, self.n_cap, self.chunk = backend, budget_bytes, model, n_cap, chunk
+        self.plain_nmax = plain_nmax  # plain requests above this n are refused (None: no bound)
+        self.refused = []
+        self.bytes_fn = bytes_fn or cb.tables_bytes
+        self.chunks = OrderedDict()  # (d, chunk index) -> _Chunk, LRU order (the chunk queries use)
+        self.building = {}           # (d, chunk index) -> _Chunk being built to replace or add
+        self.retired = []            # replaced chunks, freed once no query on them is in flight
         self.used = 0
-        self.builds = 0
-        self.plain = 0
+        self.pending = OrderedDict()  # rid -> _Req waiting for tables or queries
+        self.tickets = []            # (ticket, chunk, [(req, query column)])
+        self.plain_futs = []         # (future, req)
+        self.plain_heap = []         # (work estimate, rid) waiting for the worker
+        self.plain_busy = 0
+        self.builds = self.plain = self.launches = 0
 
-    def _bytes(self, tab):
-        return len(tab.primes) * cb.tables_bytes(tab.nmax, tab.Fmax)
+    # -- admission -----------------------------------------------------------------------------
+    def submit(self, rid, n, M, d):
+        k = cb.need(n, M, d, self.model)
+        r = _Req(rid, n, M, d, (k + self.chunk - 1) // self.chunk)
+        if not self._can_hold(r):
+            if self.plain_nmax is not None and n > self.plain_nmax:
+                self.refused.append(rid)  # a rebuild this large cannot be interrupted: not taken
+                return
+            r.plain = True
+            heapq.heappush(self.plain_heap, (k * float(n) ** 2, rid))
+        self.pending[rid] = r
 
+    def _size(self, d, c, n, M):
+        old = self.chunks.get((d, c))
+        n2 = min(self.n_cap, max(grow(n), old.nmax if old else 0))
+        F2 = max(grow(M), old.Fmax if old else 0, n2)
+        return n2, F2, self.chunk * self.bytes_fn(n2, F2)
+
+    def _can_hold(self, r):
+        """Whether the request's chunks at its size could be resident together within the budget."""
+        tot = sum(self._size(r.d, c, r.n, r.M)[2] for c in r.chunks)
+        return tot <= self.budget
+
+    # -- residency -------------------------------------------------------------------------------
     def _evict_for(self, need_bytes, keep):
         for key in list(self.chunks):
             if self.used + need_bytes <= self.budget:
                 break
-            if key in keep:
+            ch = self.chunks[key]
+            if key in keep or ch.inflight or key in self.building:
                 continue
-            tab = self.chunks.pop(key)
-            self.used -= self._bytes(tab)
-            tab.close()
+            del self.chunks[key]
+            self.used -= ch.bytes
+            self.be.free(ch.tab)
         return self.used + need_bytes <= self.budget
 
-    def _ensure(self, d, c, n, M, keep):
-        """Chunk c of degree d resident with n and M covered; False if the budget forbids it."""
-        tab = self.chunks.get((d, c))
-        if tab is not None and tab.nmax >= n and tab.Fmax >= M:
-            self.chunks.move_to_end((d, c))
-            return True
-        n2 = min(self.n_cap, max(grow(n), tab.nmax if tab else 0))
-        F2 = max(grow(M), tab.Fmax if tab else 0, n2)
-        cnt = self.chunk
-        size = cnt * cb.tables_bytes(n2, F2)
-        if tab is not None:
-            self.chunks.pop((d, c))
-            self.used -= self._bytes(tab)
-            tab.close()
-        if not self._evict_for(size, keep):
+    def _start_build(self, d, c, n, M, keep):
+        n2, F2, nbytes = self._size(d, c, n, M)
+        if not self._evict_for(nbytes, keep):
             return False
-        primes = cb.prime_range(c * cnt, cnt)
-        self.chunks[(d, c)] = self.eng.tables(primes, n2, F2, d, model=self.model)
-        self.used += size
+        primes = cb.prime_range(c * self.chunk, self.chunk)
+        tab = self.be.build(primes, n2, F2, d, self.model)
+        self.building[(d, c)] = _Chunk((d, c), tab, n2, F2, nbytes)
+        self.used += nbytes
         self.builds += 1
         return True
 
-    def round(self, reqs):
-        """Residues for a batch of requests [(id, n, M, d)] -> {id: [residue modulo prime i, i = 0, 1, ...]}
-        covering at least the request's need(n, M, d) primes (whole chunks when served resident)."""
-        res = {rid: {} for rid, _, _, _ in reqs}
-        plain = []
-        # which chunks each request needs
-        need = {rid: cb.need(n, M, d, self.model) for rid, n, M, d in reqs}
-        uses = {}
-        for rid, n, M, d in reqs:
-            for c in range((need[rid] + self.chunk - 1) // self.chunk):
-                uses.setdefault((d, c), []).append((rid, n, M))
-        keep = set(uses)
-        resident = {}
-        for (d, c), items in uses.items():
-            n = max(x[1] for x in items)
-            M = max(x[2] for x in items)
-            resident[(d, c)] = self._ensure(d, c, n, M, keep)
-        bad = {rid for (d, c), items in uses.items() if not resident[(d, c)] for rid, _, _ in items}
-        for (d, c), items in uses.items():
-            items = [x for x in items if x[0] not in bad]
-            if not items:
+    def _poll_builds(self):
+        for key, ch in list(self.building.items()):
+            if not self.be.ready(ch.tab):
                 continue
-            tab = self.chunks[(d, c)]
-            out = tab.query([(n, M) for _, n, M in items])
-            for jj, (rid, n, M) in enumerate(items):
-                res[rid][c] = out[:, jj].tolist()  # primes c*chunk .. c*chunk + chunk - 1
-        for rid, n, M, d in reqs:
-            if rid in bad:
-                plain.append((rid, n, M, d))
-        for rid, n, M, d in plain:  # no residency: rebuild for this request alone
-            ps = cb.prime_range(0, need[rid])
-            r = self.eng.residues(ps, n, d, [(n, M)], model=self.model)
-            res[rid] = {0: r[:, 0].tolist()}
+            del self.building[key]
+            ch.ready = True
+            old = self.chunks.pop(key, None)
+            if old is not None:  # replaced by a larger table: freed once its queries are back
+                self.retired.append(old)
+            self.chunks[key] = ch
+
+    def _free_retired(self):
+        keep = []
+        for ch in self.retired:
+            if ch.inflight:
+                keep.append(ch)
+            else:
+                self.used -= ch.bytes
+                self.be.free(ch.tab)
+        self.retired = keep
+
+    # -- one pass of the loop --------------------------------------------------------------------
+    def pump(self):
+        done = []
+        # results that came back
+        still = []
+        for tk, ch, items in self.tickets:
+            if not tk.done():
+                still.append((tk, ch, items))
+                continue
+            out = tk.result()
+            ch.inflight -= 1
+            for req, jj in items:
+                req.got[ch.key[1]] = out[:, jj]
+                req.sent.discard(ch.key[1])
+                if len(req.got) == len(req.chunks):
+                    done.append((req.rid, [int(x) for c in req.chunks for x in req.got[c]]))
+                    del self.pending[req.rid]
+        self.tickets = still
+        still = []
+        for fut, req in self.plain_futs:
+            if fut.done():
+                done.append((req.rid, [int(x) for x in fut.result()]))
+                del self.pending[req.rid]
+                self.plain_busy -= 1
+            else:
+                still.append((fut, req))
+        self.plain_futs = still
+        self._poll_builds()
+        # plain requests: one at a time on the worker, the least work first
+        while self.plain_heap and self.plain_busy == 0:
+            _, rid = heapq.heappop(self.plain_heap)
+            req = self.pending[rid]
+            primes = cb.prime_range(0, cb.need(req.n, req.M, req.d, self.model))
+            self.plain_futs.append((self.be.plain(primes, req.n, req.M, req.d, self.model), req))
+            self.plain_busy += 1
             self.plain += 1
-        return {rid: [x for c in sorted(v) for x in v[c]] for rid, v in res.items()}
+        # Resident requests, oldest first.  A request is provisioned when every chunk it needs is
+        # resident or being built at a size that covers it; its missing builds start together or
+        # not at all, evicting only chunks no provisioned request holds, and a request that does
+        # not fit stops the builds of the requests behind it (so the oldest always gets through
+        # once the ones ahead of it are answered, and no two requests hold parts of each other's
+        # room).  Per ready chunk, one query launch goes out for every request waiting on it.
+        wanted = {}
+        keep = set()
+        blocked = False
+        for req in self.pending.values():
+            if req.plain:
+                continue
+            missing = []
+            for c in req.chunks:
+                key = (req.d, c)
+                ch, b = self.chunks.get(key), self.building.get(key)
+                if not (ch is not None and ch.covers(req.n, req.M)) and not (b is not None and b.covers(req.n, req.M)):
+                    missing.append(c)
+            if missing:
+                if blocked or any((req.d, c) in self.building for c in missing):
+                    blocked = True  # a build of too small a size is still running: wait for it
+                else:
+                    mine = keep | {(req.d, c) for c in req.chunks}
+                    need_bytes = sum(self._size(req.d, c, req.n, req.M)[2] for c in missing)
+                    if self._evict_for(need_bytes, mine):
+                        for c in missing:
+                            self._start_build(req.d, c, req.n, req.M, mine)
+                        missing = []
+                    else:
+                        blocked = True
+            if not missing:
+                keep |= {(req.d, c) for c in req.chunks}
+            for c in req.chunks:
+                if c in req.got or c in req.sent:
+                    continue
+                key = (req.d, c)
+                ch = self.chunks.get(key)
+                if ch is not None and ch.ready and ch.covers(req.n, req.M):
+                    wanted.setdefault(key, []).append(req)
+        for key, reqs in wanted.items():
+            ch = self.chunks[key]
+            self.chunks.move_to_end(key)
+            tk = self.be.query(ch.tab, [(r.n, r.M) for r in reqs])
+            ch.inflight += 1
+            self.launches += 1
+            for r in reqs:
+                r.sent.add(key[1])
+            self.tickets.append((tk, ch, [(r, jj) for jj, r in enumerate(reqs)]))
+        self._free_retired()
+        return done
+
+    def idle(self):
+        return not self.pending
+
+    def close(self):
+        for ch in list(self.chunks.values()) + list(self.building.values()) + self.retired:
+            self.be.free(ch.tab)
+        self.chunks.clear()
+        self.building.clear()
+        self.retired = []
 
 
 # ---- host CRT workers (separate processes, started with spawn) ----
@@ -165,7 +384,6 @@ def _crt_job(residues):
 def crt_pool(max_primes, chunk=CHUNK, workers=None):
     """Process pool whose workers hold crt.PrefixCRT over the fixed list, its constants for every
     chunk-multiple prefix computed before the pool is returned."""
-    import concurrent.futures as cf
     import multiprocessing as mp
 
     workers = workers or max(1, min(16, (os.cpu_count() or 2) - 1))
@@ -178,65 +396,86 @@ def crt_pool(max_primes, chunk=CHUNK, workers=None):
     return pool
 
 
-def run(stream, engine, budget_bytes, model=cb.MODEL_SUBSET, warm=None, max_round=512, chunk=CHUNK, pool=None):
+def run(stream, backend, budget_bytes, model=cb.MODEL_SUBSET, warm=None, chunk=CHUNK, pool=None, drain_s=None,
+        bytes_fn=None, plain_nmax=None):
     """Serve a timed stream [(arrival_s, n, M, d)] in real time.  `warm`, if given, is a list of
-    (n, M, d) built before the clock starts.  Returns (latencies_s, results, stats): the latency to
-    N_bad per request, N_bad per request, and counters including the latency to residues."""
-    srv = Server(engine, budget_bytes, model, chunk=chunk)
+    (n, M, d) whose chunks are built (and waited for) before the clock starts.  After the last
+    arrival the loop runs until every request is answered, or for at most drain_s seconds.
+    plain_nmax, if given, refuses plain-path requests above that n (counted, never answered).
+    Returns (latencies_s, results, stats): latency to N_bad and N_bad per request (None when not
+    answered in time), and counters including the latency to residues."""
+    srv = Server(backend, budget_bytes, model, chunk=chunk, bytes_fn=bytes_fn, plain_nmax=plain_nmax)
     for n, M, d in warm or []:
         for c in range((cb.need(n, M, d, model) + chunk - 1) // chunk):
-            srv._ensure(d, c, n, M, set())
+            srv._start_build(d, c, n, M, set())
+    while srv.building:
+        srv._poll_builds()
+        time.sleep(0.002)
+    warm_builds = srv.builds
     own_pool = pool is None
     if own_pool:
         kmax = max([cb.need(n, M, d, model) for _, n, M, d in stream] + [1])
         pool = crt_pool(kmax, chunk)
     futs = [None] * len(stream)
-    lat, res_lat = [0.0] * len(stream), [0.0] * len(stream)
+    lat, res_lat = [None] * len(stream), [None] * len(stream)
     t0 = time.perf_counter()
-    gpu_s, rounds, i = 0.0, 0, 0
+    i = 0
+    last = stream[-1][0] if stream else 0.0
 
     def stamp(k):
         def cb_(_f):
             lat[k] = time.perf_counter() - t0 - stream[k][0]
         return cb_
 
-    while i < len(stream):
+    passes = 0
+    while True:
         now = time.perf_counter() - t0
-        if stream[i][0] > now:
-            time.sleep(min(stream[i][0] - now, 0.005))
-            continue
-        j = i
-        while j < len(stream) and stream[j][0] <= now and j - i < max_round:
-            j += 1
-        batch = [(k, stream[k][1], stream[k][2], stream[k][3]) for k in range(i, j)]
-        g0 = time.perf_counter()
-        out = srv.round(batch)
-        done = time.perf_counter() - t0
-        gpu_s += time.perf_counter() - g0
-        for k, _, _, _ in batch:
-            res_lat[k] = done - stream[k][0]
-            futs[k] = pool.submit(_crt_job, out[k])
-            futs[k].add_done_callback(stamp(k))
-        rounds += 1
-        i = j
-    results = [f.result() for f in futs]
+        while i < len(stream) and stream[i][0] <= now:
+            _, n, M, d = stream[i]
+            srv.submit(i, n, M, d)
+            i += 1
+        for rid, residues in srv.pump():
+            res_lat[rid] = time.perf_counter() - t0 - stream[rid][0]
+            futs[rid] = pool.submit(_crt_job, residues)
+            futs[rid].add_done_callback(stamp(rid))
+        passes += 1
+        if i >= len(stream) and (srv.idle() or (drain_s is not None and now > last + drain_s)):
+            break
+        if srv.idle() and i < len(stream):
+            time.sleep(max(0.0, min(stream[i][0] - now, 0.002)))
+        else:
+            time.sleep(0.0002)
     wall = time.perf_counter() - t0
-    stats = {"requests": len(stream), "rounds": rounds, "builds": srv.builds, "plain": srv.plain,
-             "resident_gb": srv.used / 1e9, "wall_s": wall, "engine_s": gpu_s,
-             "residues_latency": percentiles(res_lat)}
-    for tab in srv.chunks.values():
-        tab.close()
+    results = [f.result() if f is not None else None for f in futs]
+    unanswered = sum(1 for r in res_lat if r is None)
+    stats = {"requests": len(stream), "answered": len(stream) - unanswered, "unanswered": unanswered,
+             "refused": len(srv.refused), "loop_passes": passes, "query_launches": srv.launches,
+             "builds": srv.builds - warm_builds,
+             "warm_builds": warm_builds, "plain": srv.plain, "resident_gb": srv.used / 1e9, "wall_s": wall,
+             "residues_latency": percentiles([x for x in res_lat if x is not None])}
+    srv.close()
     if own_pool:
         pool.shutdown()
     return lat, results, stats
 
 
 def percentiles(lat):
-    a = np.sort(np.array(lat))
+    a = np.sort(np.array([x for x in lat if x is not None], dtype=float))
     if not len(a):
         return {}
     return {"p50_ms": 1e3 * float(np.percentile(a, 50)), "p99_ms": 1e3 * float(np.percentile(a, 99)),
-            "max_ms": 1e3 * float(a[-1])}
+            "max_ms": 1e3 * float(a[-1]), "count": int(len(a))}
+
+
+def bucketed(stream, lat, edges=(512, 2048, 8192, 16384)):
+    """Latency percentiles per n bucket: {"n<=512": {...}, ...}, with the unanswered count."""
+    out, lo = {}, 0
+    for e in edges:
+        ks = [k for k, (_, n, _, _) in enumerate(stream) if lo < n <= e]
+        got = [lat[k] for k in ks if lat[k] is not None]
+        out[f"{lo + 1}..{e}"] = {**percentiles(got), "requests": len(ks), "unanswered": len(ks) - len(got)}
+        lo = e
+    return out
 
 
 def main(argv=None):
@@ -248,13 +487,15 @@ def main(argv=None):
     ap.add_argument("--budget-gb", type=float, default=150)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--drain-s", type=float, default=None)
     ap.add_argument("--cold", action="store_true", help="start with no resident tables")
     a = ap.parse_args(argv)
     stream = poisson_stream(a.seconds, a.rate, a.nmin, a.nmax, a.seed)
-    warm = None if a.cold else [(a.nmax, 4 * a.nmax, d) for d in (2, 3, 4)]
-    with cb.Engine(a.device) as eng:
-        lat, _, stats = run(stream, eng, a.budget_gb * 1e9, warm=warm)
-    print({**percentiles(lat), **stats})
+    warm = None if a.cold else [(min(a.nmax, 2048), 4 * min(a.nmax, 2048), d) for d in (2, 3, 4)]
+    be = GpuBackend(a.device)
+    lat, _, stats = run(stream, be, a.budget_gb * 1e9, warm=warm, drain_s=a.drain_s)
+    be.close()
+    print({**percentiles(lat), **stats, "buckets": bucketed(stream, lat)})
     return 0
 
 

@@ -114,6 +114,21 @@ int cf_batch_graph_status(cf_batch_graph* g, void* stream);
 long cf_batch_graph_launches(const cf_batch_graph* g);
 void cf_batch_graph_destroy(cf_batch_graph* g);
 
+/* ---- geometry autotuning (no counterpart in the reference: it fixes the convolution's block
+ * size at compile time, CONV_LG, fast/cuckoo_fast.cu:518) ----
+ * The engine compiles a few geometries of the 50-bit kernel per transform length 2^lg: 2^r entries
+ * per thread in registers (the register-pass radix), threads per prime = L / 2^r, and the resident
+ * CTAs per SM its register budget targets.  cf_tune_variants describes them (the default first) and
+ * returns their number; cf_autotune times each on B primes of a table of nmax (one query (nmax,
+ * Mmax), d) through cf_residues, checks that all give the same residues, and makes the fastest
+ * the engine's choice for that length (rates[i]: primes per second of geometry i, *chosen: the
+ * index).  cf_tune_set / cf_tune_get pin or read the choice (e.g. from a cache of earlier runs).
+ * Primes below 2^62 always use the default geometry. */
+int cf_tune_variants(int lg, int* log2_entries, int* threads, int* ctas_per_sm, int cap);
+int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, int cap, int* chosen);
+int cf_tune_set(cf_engine* e, int lg, int variant);
+int cf_tune_get(const cf_engine* e, int lg);
+
 /* ---- resident tables for serving (no counterpart in the reference) ----
  * The reference rebuilds the suffix table for every run.  A served workload keeps, per (d, prime),
  * the whole table V and the factorial tables on the device, and answers later queries with

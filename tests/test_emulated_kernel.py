@@ -80,3 +80,24 @@ def test_emulated_kernel_golden_n4096(name):
     got = h.emu_residues([p for (i, p), _ in items], max(n for n, _ in qs), d, qs)
     for ((i, p), want), row in zip(items, got):
         assert row == [want[q] for q in qs], (name, i)
+
+
+@pytest.mark.parametrize("nmax,R", [(1000, 4), (2000, 3), (4000, 3), (4000, 5)])
+def test_emulated_tuning_geometries(nmax, R):
+    """The autotuner's other register-pass geometries (2^R entries per thread) compute the
+    oracle's residues: the same phase code at another thread count and radix."""
+    import ctypes
+
+    L = h.emu()
+    L.emu_residues_geo.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                   ctypes.c_int, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
+    L.emu_residues_geo.restype = ctypes.c_int
+    qs = [(nmax, 2 * nmax + 1), (nmax // 3, nmax)]
+    J = len(qs)
+    qn = (ctypes.c_int * J)(*[q[0] for q in qs])
+    qM = (ctypes.c_int * J)(*[q[1] for q in qs])
+    pr = (ctypes.c_uint64 * 1)(P0)
+    out = (ctypes.c_uint64 * J)()
+    assert L.emu_residues_geo(pr, 1, nmax, 3, 0, qn, qM, J, out, R) == 0
+    assert [int(x) for x in out] == h.oracle_residues(P0, nmax, 3, qs)
