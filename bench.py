@@ -193,7 +193,8 @@ def serving_run(device, seconds, rate=200.0, budget_gb=150.0, full_seconds=2.0, 
     * the resident range: n log-uniform in [64, 2048] for `seconds`, tables for (2048, 8192, d)
       built before the clock (they fit the budget for every d);
     * the full range the workload states, n log-uniform in [64, 16384], for `full_seconds` with
-      the same warm tables; requests above the resident range take the plain path one at a time,
+      the same warm tables; requests above the resident range (n > 2048, whose tables would evict
+      the ones that serve the rest) take the plain path one at a time,
       least work first (up to n = plain_nmax; a rebuild cannot be interrupted, so larger ones are
       refused), and the loop stops `drain_s` after the last arrival: what is not answered by then
       is counted per n bucket.
@@ -213,7 +214,7 @@ def serving_run(device, seconds, rate=200.0, budget_gb=150.0, full_seconds=2.0, 
             kmax = max(cb.need(n, M, dd) for _, n, M, dd in stream)
             pool = serve.crt_pool(kmax)
             lat, _, st = serve.run(stream, be, budget_gb * 1e9, warm=warm, pool=pool, drain_s=drain,
-                                   plain_nmax=plain_nmax if drain is not None else None)
+                                   plain_nmax=plain_nmax if drain is not None else None, resident_nmax=2048)
             pool.shutdown()
             rl = st["residues_latency"]
             nb = serve.percentiles(lat)

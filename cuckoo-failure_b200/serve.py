@@ -184,9 +184,12 @@ class Server:
     residues are complete as [(rid, residues)], residues covering at least need(n, M, d) primes."""
 
     def __init__(self, backend, budget_bytes, model=cb.MODEL_SUBSET, n_cap=16384, chunk=CHUNK, bytes_fn=None,
-                 plain_nmax=None):
+                 plain_nmax=None, resident_nmax=None):
         self.be, self.budget, self.model, self.n_cap, self.chunk = backend, budget_bytes, model, n_cap, chunk
         self.plain_nmax = plain_nmax  # plain requests above this n are refused (None: no bound)
+        # requests above this n take the plain path even when their tables would fit, so they never
+        # evict the tables that serve the requests below it (None: any that fit are made resident)
+        self.resident_nmax = resident_nmax
         self.refused = []
         self.bytes_fn = bytes_fn or cb.tables_bytes
         self.chunks = OrderedDict()  # (d, chunk index) -> _Chunk, LRU order (the chunk queries use)
@@ -204,7 +207,7 @@ class Server:
     def submit(self, rid, n, M, d):
         k = cb.need(n, M, d, self.model)
         r = _Req(rid, n, M, d, (k + self.chunk - 1) // self.chunk)
-        if not self._can_hold(r):
+        if not self._can_hold(r) or (self.resident_nmax is not None and n > self.resident_nmax):
             if self.plain_nmax is not None and n > self.plain_nmax:
                 self.refused.append(rid)  # a rebuild this large cannot be interrupted: not taken
                 return
@@ -326,7 +329,9 @@ class Server:
                 if blocked or any((req.d, c) in self.building for c in missing):
                     blocked = True  # a build of too small a size is still running: wait for it
                 else:
-                    mine = keep | {(req.d, c) for c in req.chunks}
+                    # a chunk resident at too small a size is replaced: its room counts as free once
+                    # no query on it is in flight and no request ahead holds it
+                    mine = keep | {(req.d, c) for c in req.chunks if c not in missing}
                     need_bytes = sum(self._size(req.d, c, req.n, req.M)[2] for c in missing)
                     if self._evict_for(need_bytes, mine):
                         for c in missing:
@@ -397,14 +402,16 @@ def crt_pool(max_primes, chunk=CHUNK, workers=None):
 
 
 def run(stream, backend, budget_bytes, model=cb.MODEL_SUBSET, warm=None, chunk=CHUNK, pool=None, drain_s=None,
-        bytes_fn=None, plain_nmax=None):
+        bytes_fn=None, plain_nmax=None, resident_nmax=None):
     """Serve a timed stream [(arrival_s, n, M, d)] in real time.  `warm`, if given, is a list of
     (n, M, d) whose chunks are built (and waited for) before the clock starts.  After the last
     arrival the loop runs until every request is answered, or for at most drain_s seconds.
-    plain_nmax, if given, refuses plain-path requests above that n (counted, never answered).
+    plain_nmax, if given, refuses plain-path requests above that n (counted, never answered);
+    resident_nmax, if given, sends every request above that n to the plain path.
     Returns (latencies_s, results, stats): latency to N_bad and N_bad per request (None when not
     answered in time), and counters including the latency to residues."""
-    srv = Server(backend, budget_bytes, model, chunk=chunk, bytes_fn=bytes_fn, plain_nmax=plain_nmax)
+    srv = Server(backend, budget_bytes, model, chunk=chunk, bytes_fn=bytes_fn, plain_nmax=plain_nmax,
+                 resident_nmax=resident_nmax)
     for n, M, d in warm or []:
         for c in range((cb.need(n, M, d, model) + chunk - 1) // chunk):
             srv._start_build(d, c, n, M, set())

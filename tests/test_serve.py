@@ -168,6 +168,33 @@ def test_requests_are_answered_while_a_build_and_a_plain_request_are_in_flight()
         assert pc.crt(got[rid])[0] == alone(n, M, d), rid
 
 
+def test_a_chunk_too_small_is_replaced_when_old_and_new_do_not_fit_together():
+    """A request that needs a resident chunk rebuilt larger, with room for the larger chunk but not
+    for both: the small one is freed for it (no query on it in flight), and the request is answered."""
+    be = OracleBackend()
+    bytes_fn = lambda nmax, Fmax: 15 if nmax <= 64 else 20  # per prime: 480 / 640 bytes per chunk of 32
+    srv = serve.Server(be, 1000, chunk=32, bytes_fn=bytes_fn)
+    srv.submit(0, 20, 50, 2)
+    r0 = pump_until_idle(srv)[0]
+    assert srv.chunks[(2, 0)].nmax == 64
+    srv.submit(1, 70, 150, 2)  # one chunk of 32 primes at n = 80
+    r1 = pump_until_idle(srv)[1]
+    pc = crt.PrefixCRT(cb.prime_range(0, 64))
+    assert pc.crt(r0)[0] == alone(20, 50, 2) and pc.crt(r1)[0] == alone(70, 150, 2)
+    assert srv.chunks[(2, 0)].nmax == 80 and srv.used <= 1000 and srv.plain == 0
+
+
+def test_requests_above_the_resident_range_take_the_plain_path():
+    be = OracleBackend()
+    srv = serve.Server(be, 10**12, chunk=8, resident_nmax=24)
+    srv.submit(0, 20, 50, 2)
+    srv.submit(1, 30, 70, 2)
+    got = pump_until_idle(srv)
+    pc = crt.PrefixCRT(cb.prime_range(0, 64))
+    assert pc.crt(got[0])[0] == alone(20, 50, 2) and pc.crt(got[1])[0] == alone(30, 70, 2)
+    assert srv.plain == 1 and all(k[0] == 2 and ch.nmax <= 64 for k, ch in srv.chunks.items())
+
+
 def test_prefix_crt_equals_pairwise_crt():
     import random
 
@@ -188,7 +215,7 @@ def test_served_results_equal_alone_on_gpu():
     be = serve.GpuBackend(0)
     try:
         budget = 6 * 64 * cb.tables_bytes(320, 1280)
-        lat, res, stats = serve.run(stream, be, budget, chunk=64)
+        lat, res, stats = serve.run(stream, be, budget, chunk=64, drain_s=180)  # a stall fails, never hangs
         with cb.Engine(0) as eng:
             for (t, n, M, d), x in zip(stream, res):
                 ps = cb.prime_range(0, cb.need(n, M, d))
