@@ -81,8 +81,9 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "need queries with 8 <= max n < 2^%d\n", cfh::TWO_ADIC);
         return 2;
     }
-    if (cf_transform_length((uint64_t)nmax) > 16384) {
-        std::fprintf(stderr, "this build handles tables up to n = 16384 (got %d)\n", nmax);
+    if (cf_transform_length((uint64_t)nmax) > (bits == 62 ? 16384 : 65536)) {
+        std::fprintf(stderr, "this build handles tables up to n = %d with %d-bit primes (got %d)\n",
+                     bits == 62 ? 16384 : 65536, bits, nmax);
         return 2;
     }
 

@@ -44,8 +44,49 @@ KInfo kernel_for(int lg, bool wide) {
         case 12: return cf_kinfo_lg12();
         case 13: return cf_kinfo_lg13();
         case 14: return cf_kinfo_lg14();
+        case 15: return cf_kinfo_lg15_c4();
+        case 16: return cf_kinfo_lg16_c16();
         default: return KInfo{nullptr, 0, 0, 0};
     }
+}
+// The cluster sizes compiled for transform length 2^lg (15, 16), smallest first.
+static int cluster_variants(int lg, KInfo* v) {
+    if (lg == 15) return v[0] = cf_kinfo_lg15_c4(), v[1] = cf_kinfo_lg15_c8(), 2;
+    if (lg == 16) return v[0] = cf_kinfo_lg16_c8(), v[1] = cf_kinfo_lg16_c16(), 2;
+    return 0;
+}
+// Clusters of the kernel ki (at smem bytes of dynamic shared memory) the device runs at once.
+static int resident_clusters(const KInfo& ki, size_t smem, cudaStream_t s) {
+    if (cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    if (ki.cluster > 8 && cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+        return 0;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)ki.cluster, at[0].val.clusterDim.y = 1, at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)ki.cluster), cfg.blockDim = dim3((unsigned)ki.threads), cfg.dynamicSmemBytes = smem;
+    cfg.stream = s, cfg.attrs = at, cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, (const void*)ki.fn, &cfg) != cudaSuccess) return 0;
+    return n;
+}
+// The cluster size for a launch of nb primes at transform length 2^lg: the least time per prime,
+// taken as waves (ceil(nb / resident clusters)) over CTAs per prime; ties go to the smaller cluster.
+static KInfo pick_cluster(const cf_engine* e, int lg, int nb, int J, cudaStream_t s) {
+    KInfo v[4];
+    const int k = cluster_variants(lg, v);
+    const int forced = lg > MAX_LG ? e->cluster_pick[lg - MAX_LG - 1] : -1;
+    if (forced >= 0 && forced < k) return v[forced];
+    KInfo best = kernel_for(lg);
+    double best_cost = 0;
+    for (int i = 0; i < k; ++i) {
+        const int rc = resident_clusters(v[i], v[i].smem_for(J), s);
+        if (rc < 1) continue;
+        const double cost = (double)((nb + rc - 1) / rc) / v[i].cluster;
+        if (best_cost == 0 || cost < best_cost) best = v[i], best_cost = cost;
+    }
+    return best;
 }
 int cf_kvariants_lg10(KInfo* out, int cap);
 int cf_kvariants_lg11(KInfo* out, int cap);
@@ -85,10 +126,13 @@ struct Plan {
 // The kernel this engine runs for the plan and the workspace layout its geometry needs (the
 // pass-0 twiddle tables follow the entries per thread); again whenever wide or F changes.
 static int finalize(cf_engine* e, Plan& pl) {
+    if (pl.wide && pl.lg > MAX_LG)
+        return fail(e, CF_ERR_UNSUPPORTED, "primes of 2^50 and above run with transforms up to 2^14 (nmax <= 16384)");
     pl.ki = kernel_of(e, pl.lg, pl.wide);
     if (!pl.ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     const int nw = pl.ki.threads >= 32 ? pl.ki.threads / 32 : 1;
-    pl.lay = make_layout(pl.nmax, pl.F, 1 << pl.lg, pl.J, nw, pl.ki.r);
+    // cluster kernels: row sums for the largest cluster, so any cluster size can run the layout
+    pl.lay = make_layout(pl.nmax, pl.F, 1 << pl.lg, pl.J, nw, pl.ki.r, pl.lg > MAX_LG ? MAX_CLUSTER : 1);
     pl.ws_words = pl.lay.total;
     return CF_OK;
 }
@@ -107,7 +151,9 @@ static int plan(cf_engine* e, int nmax, int d, int model, const int* qn, const i
     const u64 L = cfh::transform_length((u64)nmax);
     int lg = 0;
     while ((1ull << lg) < L) ++lg;
-    if (lg > MAX_LG) return fail(e, CF_ERR_UNSUPPORTED, "transform length above 2^14 (nmax > 16384) is not supported by this build");
+    if (e && e->min_lg > lg) lg = e->min_lg;
+    if (lg > MAX_LG_CLUSTER)
+        return fail(e, CF_ERR_UNSUPPORTED, "transform length above 2^16 (nmax > 65536) is not supported by this build");
     pl.lg = lg;
     pl.F = F;
     pl.d0 = model == CF_MODEL_SUBSET ? d : 1;
@@ -178,9 +224,11 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
                         u64* d_out, cudaStream_t s, u64* keep = nullptr, size_t keep_words = 0, bool fixed_ws = false,
                         int* err = nullptr) {
     if (!err) err = e->d_err;
-    const KInfo ki = pl.ki;
+    KInfo ki = pl.ki;
     if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
-    const size_t smem = ki.smem_for(J);
+    if (ki.cluster > 1 && keep) return fail(e, CF_ERR_UNSUPPORTED, "resident tables are built up to nmax = 16384");
+    if (ki.cluster > 1) ki = pick_cluster(e, pl.lg, B, J, s);  // refined per chunk below
+    size_t smem = ki.smem_for(J);
     int rc0 = check_smem(e, smem, J);
     if (rc0) return rc0;
     CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -221,7 +269,26 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
         kp.err = err;
         kp.keep = keep ? keep + (size_t)at * keep_words : nullptr;
         kp.keep_words = keep_words;
-        ki.fn<<<nb, ki.threads, smem, s>>>(kp);
+        if (ki.cluster > 1) {  // one cluster of ki.cluster CTAs per prime
+            ki = pick_cluster(e, pl.lg, nb, J, s);
+            smem = ki.smem_for(J);
+            rc0 = check_smem(e, smem, J);
+            if (rc0) return rc0;
+            CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                    "shared memory attribute");
+            if (ki.cluster > 8)
+                CF_CUDA(cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+                        "cluster size attribute");
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute att[1];
+            att[0].id = cudaLaunchAttributeClusterDimension;
+            att[0].val.clusterDim.x = (unsigned)ki.cluster, att[0].val.clusterDim.y = 1, att[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3((unsigned)(nb * ki.cluster)), cfg.blockDim = dim3((unsigned)ki.threads);
+            cfg.dynamicSmemBytes = smem, cfg.stream = s, cfg.attrs = att, cfg.numAttrs = 1;
+            CF_CUDA(cudaLaunchKernelEx(&cfg, ki.fn, kp), "cluster kernel launch");
+        } else {
+            ki.fn<<<nb, ki.threads, smem, s>>>(kp);
+        }
         CF_CUDA(cudaGetLastError(), "kernel launch");
         ++e->launches;
     }
@@ -299,9 +366,9 @@ uint64_t cf_workspace_bytes(int nmax, int Mmax, int J) {
     const u64 L = cfh::transform_length((u64)nmax);
     int lg = 0;
     while ((1ull << lg) < L) ++lg;
-    if (lg > MAX_LG) return 0;
+    if (lg > MAX_LG_CLUSTER) return 0;
     const KInfo ki = kernel_for(lg);
-    return 8 * make_layout(nmax, F, (int)L, J, ki.threads >= 32 ? ki.threads / 32 : 1, ki.r).total;
+    return 8 * make_layout(nmax, F, (int)L, J, ki.threads >= 32 ? ki.threads / 32 : 1, ki.r, lg > MAX_LG ? MAX_CLUSTER : 1).total;
 }
 
 // ---- resident tables (serving) ----
@@ -341,6 +408,7 @@ static int tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, i
     rc = check_primes(e, primes, B, pl);  // and the layout for that F
     if (rc) return rc;
     if (pl.wide) return fail(e, CF_ERR_UNSUPPORTED, "resident tables hold primes below 2^50");
+    if (pl.lg > MAX_LG) return fail(e, CF_ERR_UNSUPPORTED, "resident tables are built up to nmax = 16384");
     CF_CUDA(cudaSetDevice(e->device), "set device");
     cf_tables* t = new cf_tables();
     t->device = e->device, t->n = nmax, t->F = pl.F, t->d = d, t->d0 = pl.d0, t->model = model, t->B = B;
@@ -486,6 +554,12 @@ void cf_tables_free(cf_tables* t) {
 int cf_engine_set_max_ctas(cf_engine* e, int n) {
     if (!e || n < 0) return CF_ERR_ARG;
     e->max_ctas = n;
+    return CF_OK;
+}
+
+int cf_engine_set_transform_lg(cf_engine* e, int lg) {
+    if (!e || lg < 0 || lg > MAX_LG_CLUSTER) return CF_ERR_ARG;
+    e->min_lg = lg;
     return CF_OK;
 }
 
@@ -656,9 +730,9 @@ long cf_batch_graph_launches(const cf_batch_graph* g) { return g ? g->launches :
 // ---- autotuning of the kernel geometry ----
 
 int cf_tune_variants(int lg, int* log2_entries, int* threads, int* ctas_per_sm, int cap) {
-    if (lg < 0 || lg > MAX_LG || cap < 0) return -1;
+    if (lg < 0 || lg > MAX_LG_CLUSTER || cap < 0) return -1;
     KInfo v[MAX_VARIANTS];
-    const int k = variants_for(lg, v, MAX_VARIANTS);
+    const int k = lg > MAX_LG ? cluster_variants(lg, v) : variants_for(lg, v, MAX_VARIANTS);
     for (int i = 0; i < k && i < cap; ++i) {
         if (log2_entries) log2_entries[i] = v[i].r;
         if (threads) threads[i] = v[i].threads;
@@ -668,6 +742,12 @@ int cf_tune_variants(int lg, int* log2_entries, int* threads, int* ctas_per_sm, 
 }
 
 int cf_tune_set(cf_engine* e, int lg, int variant) {
+    if (e && lg > MAX_LG && lg <= MAX_LG_CLUSTER) {  // a cluster size, or -1: chosen per batch
+        KInfo v[4];
+        if (variant < -1 || variant >= cluster_variants(lg, v)) return CF_ERR_ARG;
+        e->cluster_pick[lg - MAX_LG - 1] = variant;
+        return CF_OK;
+    }
     if (!e || lg < 0 || lg > MAX_LG || variant < 0) return CF_ERR_ARG;
     KInfo v[MAX_VARIANTS];
     if (variant >= variants_for(lg, v, MAX_VARIANTS)) return CF_ERR_ARG;
@@ -675,7 +755,10 @@ int cf_tune_set(cf_engine* e, int lg, int variant) {
     return CF_OK;
 }
 
-int cf_tune_get(const cf_engine* e, int lg) { return e && lg >= 0 && lg <= MAX_LG ? e->tuned[lg] : -1; }
+int cf_tune_get(const cf_engine* e, int lg) {
+    if (e && lg > MAX_LG && lg <= MAX_LG_CLUSTER) return e->cluster_pick[lg - MAX_LG - 1];
+    return e && lg >= 0 && lg <= MAX_LG ? e->tuned[lg] : -1;
+}
 
 int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, int cap, int* chosen) {
     if (!e || B < 1 || nmax < 1) return CF_ERR_ARG;
@@ -683,7 +766,7 @@ int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, i
     const u64 L = cfh::transform_length((u64)nmax);
     int lg = 0;
     while ((1ull << lg) < L) ++lg;
-    if (lg > MAX_LG) return fail(e, CF_ERR_UNSUPPORTED, "transform length above 2^14");
+    if (lg > MAX_LG) return fail(e, CF_ERR_UNSUPPORTED, "autotuning covers transforms up to 2^14; above, the cluster size follows the batch");
     KInfo v[MAX_VARIANTS];
     const int k = variants_for(lg, v, MAX_VARIANTS);
     const std::vector<u64> primes = cfh::prime_range(0, B);

@@ -34,7 +34,13 @@ cfb::KInfo cf_kinfo_lg13_w();
 cfb::KInfo cf_kinfo_lg14_w();
 // The kernel for transform length 2^lg: primes below 2^50, or (wide) below 2^62 (engine.cu).
 cfb::KInfo kernel_for(int lg, bool wide = false);
-constexpr int MAX_LG = 14;
+cfb::KInfo cf_kinfo_lg15_c4();
+cfb::KInfo cf_kinfo_lg15_c8();
+cfb::KInfo cf_kinfo_lg16_c8();
+cfb::KInfo cf_kinfo_lg16_c16();
+constexpr int MAX_LG = 14;          // one CTA per prime (every entry point)
+constexpr int MAX_LG_CLUSTER = 16;  // a cluster of CTAs per prime (cf_residues and its forms, primes below 2^50)
+constexpr int MAX_CLUSTER = 16;     // the largest cluster a layout provides row sums for
 struct cf_engine;
 // CF_OK if a launch with J queries fits the device's shared memory per block (engine.cu)
 int check_smem(cf_engine* e, size_t smem, int J);
@@ -58,6 +64,8 @@ struct cf_engine {
     int prime_bits = 50;  // for cf_residues_async, whose primes are not read on the host
     int max_ctas = 0;     // CTAs (primes) per launch at most, 0 = no cap
     int tuned[MAX_LG + 1] = {};  // geometry (index into the compiled variants) per transform length
+    int min_lg = 0;              // transforms of at least 2^min_lg entries (cf_engine_set_transform_lg)
+    int cluster_pick[MAX_LG_CLUSTER - MAX_LG] = {-1, -1};  // forced cluster variant per length above 2^14 (-1: by batch)
     std::string err;
 };
 

@@ -13,29 +13,55 @@ namespace cfb {
 template <class G>
 struct DevExec {
     Regs<G> r;
+    // this CTA's rank in its cluster (0 without clusters)
+    __device__ __forceinline__ int rank() const {
+        if constexpr (G::C == 1) return 0;
+        else {
+            u32 v;
+            asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(v));
+            return (int)v;
+        }
+    }
+    // f(t) with t the thread's index in the cluster's T threads (its CTA's CT threads without clusters)
     template <class F>
     __device__ __forceinline__ void each(F&& f) {
-        f((int)threadIdx.x, r);
+        if constexpr (G::C == 1) f((int)threadIdx.x, r);
+        else f(rank() * G::CT + (int)threadIdx.x, r);
     }
     template <class F>
     __device__ __forceinline__ void single(F&& f) {
         if (threadIdx.x == 0) f();
     }
     __device__ __forceinline__ void sync() { __syncthreads(); }
+    // Barrier of all the cluster's threads; orders their shared (local and distributed) and global
+    // memory accesses at cluster scope.
+    __device__ __forceinline__ void cluster_sync() {
+        asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+        asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
+    // Store into CTA `rk`'s shared memory at the offset `p` has in this CTA's (distributed shared memory).
+    __device__ __forceinline__ void st_remote(u64* p, int rk, u64 v) const {
+        u32 ra;
+        asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"((u32)__cvta_generic_to_shared(p)), "r"(rk));
+        asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(ra), "l"(v) : "memory");
+    }
     __device__ __forceinline__ void set_error(int* err, int code) { atomicCAS(err, 0, code); }
-    // Tensor memory: one warp allocates all 512 columns for the CTA (one CTA per SM uses it);
+    // Tensor memory: one warp allocates the CTA's columns (one CTA per SM uses it): all 512, or
+    // for a cluster's CTA the 4 E CT / 128 its threads use (a power of two, at least 32);
     // thread t of warp w owns lane 32 (w % 4) + (t % 32), columns 4E (w / 4) + [0, 4E): E pairs.
+    static constexpr u32 TM_COLS = G::C == 1 ? 512 : (4 * G::E * (G::CT / 128) < 32 ? 32 : 4 * G::E * (G::CT / 128));
+    static_assert((TM_COLS & (TM_COLS - 1)) == 0 && TM_COLS <= 512, "tensor memory columns: a power of two up to 512");
     __device__ __forceinline__ void tmem_alloc(u32* slot) {
         if ((threadIdx.x >> 5) == 0) {
             asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                             (u32)__cvta_generic_to_shared(slot)), "r"(512));
+                             (u32)__cvta_generic_to_shared(slot)), "r"(TM_COLS));
             asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
         }
         tmem_sync();
     }
     __device__ __forceinline__ void tmem_free(u32 base) {
         tmem_sync();
-        if ((threadIdx.x >> 5) == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(512));
+        if ((threadIdx.x >> 5) == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(TM_COLS));
     }
     __device__ __forceinline__ void tmem_sync() {
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -171,11 +197,12 @@ struct RFor {
 typedef void (*kfn_t)(KParams);
 struct KInfo {
     kfn_t fn;
-    int threads;
+    int threads;  // per CTA
     size_t smem;  // fixed dynamic shared memory; a launch with J queries adds 8 J (threads / 32)
     int r;        // log2 of the entries per thread
     qfn_t qfn;    // the work-queue form (the default geometry only)
     int mb;       // resident CTAs per SM the kernel is compiled for
+    int cluster = 1;  // CTAs per prime (a thread-block cluster when above 1)
     size_t smem_for(int J) const { return smem + (size_t)8 * J * (threads >= 32 ? threads / 32 : 1); }
 };
 // W selects the kernel for primes below 2^62 (otherwise below 2^50).
@@ -184,6 +211,21 @@ inline KInfo kinfo() {
     typedef Geo<LG, RFor<LG>::R> G;
     return KInfo{&k_suffix<LG, RFor<LG>::R, W>, G::T, Smem<G>::BYTES, RFor<LG>::R, &k_suffix_queue<LG, RFor<LG>::R, W>,
                  MinBlocks<LG>::v};
+}
+// Transform lengths above 2^14 (tables above n = 16384, primes below 2^50): one prime per cluster of
+// 2^LC CTAs, one CTA per SM, launched with that cluster size (CTA b 2^LC + c is CTA c of prime b).
+template <int LG, int R, int LC>
+__global__ void __launch_bounds__(Geo<LG, R, LC>::CT, 1) k_suffix_cl(KParams kp) {
+    typedef Geo<LG, R, LC> G;
+    extern __shared__ __align__(16) u64 smem[];
+    DevExec<G> ex;
+    PrimeRun<G, DevExec<G>, false> pr(ex, kp, (int)blockIdx.x >> LC, smem);
+    pr.run();
+}
+template <int LG, int LC>
+inline KInfo kinfo_cluster() {
+    typedef Geo<LG, 4, LC> G;
+    return KInfo{&k_suffix_cl<LG, 4, LC>, G::CT, Smem<G>::BYTES, 4, nullptr, 1, G::C};
 }
 // Another geometry of the 50-bit kernel (autotuning candidates): 2^R entries per thread, MB CTAs per SM.
 template <int LG, int R, int MB>

@@ -160,13 +160,29 @@ constexpr int WIN_K = CF_WIN_K;    // units in flight beyond the current one
 // Transform geometry: L = 2^LG entries, T threads holding E = 2^R entries each.  The LG levels
 // are done in passes of R levels (the last pass may have fewer); between passes the entries go
 // through shared memory.
-template <int LG_, int R_>
+//
+// Clusters (LC > 0): the T threads are spread over C = 2^LC CTAs of CT = T / C threads, thread t
+// being thread t % CT of the cluster's CTA t / CT.  Pass 0 holds index t + jT in slot j (a
+// column of every one of the E blocks of L / E entries); after it every later pass works inside one
+// block, and CTA c holds blocks c E / C .. (c + 1) E / C - 1 (E >= C), i.e. the indices
+// [c L / C, (c + 1) L / C).  So the entries cross between CTAs only after the first forward pass
+// and before the last inverse pass, through distributed shared memory.
+template <int LG_, int R_, int LC_ = 0>
 struct Geo {
-    static constexpr int LG = LG_, R = R_;
+    static constexpr int LG = LG_, R = R_, LC = LC_;
     static constexpr int L = 1 << LG, E = 1 << R, T = 1 << (LG - R);
+    static constexpr int C = 1 << LC, CT = T >> LC, LCN = L >> LC;  // CTAs, threads and entries per CTA
     static constexpr int NP = (LG + R - 1) / R;  // number of passes
     static constexpr int SWZ = R > 4 ? R : 4;    // shared-memory swizzle shift
-    static constexpr int NW = (T + 31) / 32;     // warps
+    static constexpr int NW = (CT + 31) / 32;    // warps per CTA
+    static_assert(C == 1 || (E >= C && CT % 128 == 0 && NP >= 3), "a cluster needs E >= C, whole warp quarters and 3 passes");
+    // Forward transform for primes below 2^50 (reduction-free, bounds below): up to 2^14 entries the
+    // sums grow through every level; above, pass 0's outputs are reduced lazily to [0, 4p) (at the
+    // exchange between CTAs) and the later levels grow from there.  flvl(s): the s' with level s's
+    // inputs below 2^s' p.
+    static constexpr int FRED = LG > 14 ? R : 0;
+    CF_HD static constexpr int flvl(int s) { return FRED && s >= FRED ? s - FRED + 2 : s; }
+    static_assert(LG <= 14 || LG - FRED + 2 <= 14, "forward bounds need 2^14 p < 2^64");
     CF_HD static constexpr int pass_b(int p) { return LG - (p + 1) * R > 0 ? LG - (p + 1) * R : 0; }
     CF_HD static constexpr int pass_r(int p) { return LG - p * R - pass_b(p); }
     // index of the entry held in slot j by thread t during pass p
@@ -186,6 +202,9 @@ struct Geo {
         return s <= R_LAST ? (u64)4 << s : ((u64)4 << R_LAST) + 4 * (u64)(s - R_LAST);
     }
     static constexpr u64 INV_OUT = inv_bound(LG);  // bound of the inverse transform's outputs
+    // Bound (multiple of p) of the stage-2 product p e[p] with the companion p floor(2^64 / p): the
+    // quotient estimate loses at most p x / 2^64 < INV_OUT 2^(LG - 14) more for p <= L, P < 2^50.
+    static constexpr u64 PE_B = LG <= 14 ? INV_OUT + 4 : (INV_OUT << (LG - 14)) + 5;
 };
 
 CF_HD u64 red2(u64 x, u64 m) { return x >= m ? x - m : x; }  // [0, 2m) -> [0, m)
@@ -236,8 +255,9 @@ CF_HD size_t lay_take(size_t& at, size_t cnt) {
     at += (cnt + 31) & ~(size_t)31;
     return r;
 }
-// nw = warps per CTA: query partial sums are kept per warp.
-CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R) {
+// nw = warps per CTA: query partial sums are kept per warp.  C: CTAs per prime (each keeps its own
+// row sums of the queries).
+CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R, int C = 1) {
     Layout o;
     size_t at = 0;
     o.V = lay_take(at, block_count(n) << 8);         // rows p = 1..n, entries w = 1..p-1 (blocks)
@@ -251,7 +271,7 @@ CF_HD Layout make_layout(int n, int F, int L, int J, int nw, int R) {
     o.Gm = lay_take(at, 2 * ((size_t)n + 1));     // (g(v), 1/g(v)) in Montgomery form, v = 0 .. n
     for (int l = 0; l < 8; ++l) o.WL[l] = l < R ? lay_take(at, 2 * (((size_t)L >> (l + 1)) + 1)) : 0;  // pairs
     o.hat = lay_take(at, 2 * (size_t)L);          // pairs: spectrum of the kernel 1/t, times 1/L
-    o.ps = lay_take(at, (size_t)J * (n + 1));  // [J][n+1] row sums per query
+    o.ps = lay_take(at, (size_t)C * J * (n + 1));  // [C][J][n+1] row sums per query (per CTA of the prime)
     (void)nw;
     o.total = at;
     return o;
@@ -298,16 +318,22 @@ enum { KERR_NONE = 0, KERR_NO_ROOT = 1 };
 // Shared memory per CTA, in 64-bit words.
 template <class G>
 struct Smem {
-    static constexpr int X = 0;                       // [L] transform exchange (swizzled)
-    static constexpr int RED = G::L;                  // [2T + 64] reduction and scan scratch
-    static constexpr int MISC = RED + 2 * G::T + 64;  // [16] modulus constants and scalars
+    // [L] transform exchange by index (swizzled); a CTA of a cluster holds the LCN indices of its
+    // blocks there (by index - c LCN) and, at X0, pass 0's column layout: slot j of thread t at
+    // X0 + t % CT + j CT, written by the CTAs that finish the inverse transform's upper levels
+    static constexpr int X = 0;
+    static constexpr int X0 = G::C > 1 ? G::LCN : 0;
+    static constexpr int RED = G::C > 1 ? 2 * G::LCN : G::L;  // [2 CT + 64] reduction and scan scratch
+    static constexpr int MISC = RED + 2 * G::CT + 64;        // [16] modulus constants and scalars
     static constexpr int TWS = MISC + 16;             // pairs w^(k 2^R), k = 0 .. L/2^(R+1): passes >= 1
     static constexpr int TWS_N = (G::L >> (G::R + 1)) + 1;
     // [2][PW_STRIDE] powers of 1/g(v) and g(v) for stage 2, rebuilt every step (power_tables)
     static constexpr int PW = TWS + 2 * TWS_N;
     static constexpr int PW_STRIDE = 104;
     static constexpr int WORDS = PW + 2 * PW_STRIDE;
-    static constexpr size_t BYTES = (size_t)WORDS * 8;
+    // A cluster's CTAs take more than half an SM's shared memory, so no two share an SM (a CTA
+    // waiting for tensor memory held by another CTA of its own cluster would never get it).
+    static constexpr size_t BYTES = G::C > 1 && WORDS * 8 < 120 * 1024 ? 120 * 1024 : (size_t)WORDS * 8;
     // [J][NW] per-warp query partial sums of the current row, after the fixed part (the launch's
     // dynamic shared memory is BYTES + 8 J NW)
     static constexpr int QS = WORDS;
@@ -332,26 +358,43 @@ struct Regs {
 template <class G, class X, bool W = false>
 struct PrimeRun {
     static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP, NW = G::NW;
-    static_assert(W || G::LG <= 14, "reduction-free forward transform needs 2^LG p < 2^64");
+    static constexpr int C = G::C, CT = G::CT, LCN = G::LCN;  // a cluster of C CTAs of CT threads per prime
+    static_assert(W || G::LG <= 14 || G::FRED, "reduction-free forward transform needs 2^LG p < 2^64");
+    static_assert(!W || C == 1, "primes below 2^62 run on one CTA per prime");
     static_assert(NP > 1, "layout 0 must hold index t + jT in slot j of thread t");
     // L = 2^14 (1024 threads x 16 entries): the kernel spectrum lives in tensor memory, each
     // thread's 16 (value, companion) pairs in its own 64 columns (all 512 columns of the SM's 128
-    // lanes); smaller transforms, several CTAs to an SM, read it from global.
-    static constexpr bool TM = (T == 1024 && E == 16) || (T == 512 && E == 32);
+    // lanes); smaller transforms, several CTAs to an SM, read it from global.  A cluster's CTAs
+    // (one per SM) keep their blocks' part of it in 4 E CT / 128 columns.
+    static constexpr bool TM = (T == 1024 && E == 16) || (T == 512 && E == 32) || (C > 1 && 4 * E * (CT / 128) <= 512);
     // Constants in flight and units in flight of the hot loops.  At 1024 threads (64 registers each)
     // the shallowest schedule spills least and measured fastest (49.7 vs 48.9 prime-residues/s).
-    static constexpr int PD = T >= 1024 ? 1 : PIPE_D, WK = T >= 1024 ? 1 : WIN_K;
+    static constexpr int PD = CT >= 1024 ? 1 : PIPE_D, WK = CT >= 1024 ? 1 : WIN_K;
     X& ex;
     const KParams& kp;
     int b;      // prime index within the batch
     u64* base;  // this prime's workspace
     u64* sm;    // shared memory
     u64 P;
+    int rank_;  // this CTA's rank in its cluster
 
     // bi: the prime's index in kp.primes (and its output row); slot: its workspace slot (bi if < 0)
     CF_HD PrimeRun(X& e, const KParams& k, int bi, u64* smem, int slot = -1) : ex(e), kp(k), b(bi), sm(smem) {
         P = kp.primes[b];
         base = kp.ws + (size_t)(slot < 0 ? bi : slot) * kp.ws_words;
+        rank_ = ex.rank();
+    }
+    CF_HD int rank() const {
+        if constexpr (C == 1) return 0;
+        else return rank_;
+    }
+    CF_HD static int lt(int t) {  // thread index within the CTA
+        if constexpr (C == 1) return t;
+        else return t & (CT - 1);
+    }
+    CF_HD void csync() {  // barrier of the whole cluster (of the CTA alone when C = 1)
+        if constexpr (C == 1) ex.sync();
+        else ex.cluster_sync();
     }
     // workspace tables (offsets live in the kernel parameters, so these hold no registers)
     CF_HD u64* V() const { return base + kp.lay.V; }
@@ -366,7 +409,8 @@ struct PrimeRun {
     CF_HD u64* WL(int l) const { return base + kp.lay.WL[l]; }
     CF_HD u64* tws() const { return sm + Smem<G>::TWS; }
     CF_HD u64* hat() const { return base + kp.lay.hat; }
-    CF_HD u64* ps() const { return base + kp.lay.ps; }
+    CF_HD u64* ps() const { return ps_of(rank()); }
+    CF_HD u64* ps_of(int c) const { return base + kp.lay.ps + (size_t)c * kp.J * (kp.n + 1); }  // CTA c's row sums
     CF_HD u64* misc() const { return sm + Smem<G>::MISC; }
     CF_HD Mod md() const {  // modulus constants, kept in shared memory
         const u64* m = misc();
@@ -491,7 +535,7 @@ struct PrimeRun {
                         x[j1] = red2(a + c, P2);
                     }
                 } else if constexpr (FWD) {  // inputs below 2^s p, outputs below 2^(s+1) p
-                    constexpr int s = PL::lvl(q);
+                    constexpr int s = G::flvl(PL::lvl(q));
                     const u64 a = x[j0], c = x[j1];
                     x[j0] = a + c;
                     const u64 dd = a - c + (P << s);
@@ -524,21 +568,57 @@ struct PrimeRun {
     CF_HD void fwd_pass(int t, u64 (&x)[E]) const { pass<PASS, true>(t, x); }
     template <int PASS>
     CF_HD void inv_pass(int t, u64 (&x)[E]) const { pass<PASS, false>(t, x); }
-    template <int PASS>
-    CF_HD void to_smem(int t, const u64 (&x)[E]) const {
+    // Entries to shared memory by index.  In a cluster, pass 0's outputs (forward) go to the CTA
+    // whose block holds them, reduced to [0, 4p) when the forward bounds need it (Geo::FRED), and
+    // with TO_L0 the inverse transform's pass-1 outputs go to the CTA that holds them in pass 0.
+    template <int PASS, bool TO_L0 = false>
+    CF_HD void to_smem(int t, u64 (&x)[E]) const {
         pin_int(t);  // recompute the addresses rather than keep the loads' 32 addresses live across the pass
+        if constexpr (C > 1 && PASS == 0) {
 #pragma unroll
-        for (int j = 0; j < E; ++j) sm[G::swz(G::idx(PASS, t, j))] = x[j];
+            for (int j = 0; j < E; ++j) {
+                const int i = G::idx(0, t, j);
+                const u64 v = (G::FRED && !W) ? shoup_mul_lazy(x[j], 1, misc()[MI_ONEQ], P) : x[j];
+                ex.st_remote(sm + G::swz(i & (LCN - 1)), i / LCN, v);
+            }
+        } else if constexpr (C > 1 && TO_L0) {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                const int i = G::idx(PASS, t, j);
+                ex.st_remote(sm + Smem<G>::X0 + (i & (CT - 1)) + (i / T) * CT, (i & (T - 1)) / CT, x[j]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                const int i = G::idx(PASS, t, j);
+                if constexpr (G::FRED && !W && PASS == 0) x[j] = shoup_mul_lazy(x[j], 1, misc()[MI_ONEQ], P);
+                sm[G::swz(C > 1 ? i & (LCN - 1) : i)] = x[j];
+            }
+        }
     }
     template <int PASS>
     CF_HD void from_smem(int t, u64 (&x)[E]) const {
+        if constexpr (C > 1 && PASS == 0) {
 #pragma unroll
-        for (int j = 0; j < E; ++j) x[j] = sm[G::swz(G::idx(PASS, t, j))];
+            for (int j = 0; j < E; ++j) x[j] = sm[Smem<G>::X0 + lt(t) + j * CT];
+        } else {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                const int i = G::idx(PASS, t, j);
+                x[j] = sm[G::swz(C > 1 ? i & (LCN - 1) : i)];
+            }
+        }
+    }
+    // the barrier before pass PASS reads shared memory: the cluster's at the exchanges
+    template <int PASS, bool FWD>
+    CF_HD void pass_sync() {
+        if constexpr (C > 1 && ((FWD && PASS == 1) || (!FWD && PASS == 0))) ex.cluster_sync();
+        else ex.sync();
     }
 
     template <int PASS>
     CF_HD void fwd_chain() {  // forward passes PASS .. NP-1, pointwise, last inverse pass (PASS >= 1)
-        ex.sync();
+        pass_sync<PASS, true>();
         ex.each([&](int t, Regs<G>& rg) CF_INL {
             from_smem<PASS>(t, rg.x);
             fwd_pass<PASS>(t, rg.x);
@@ -546,40 +626,40 @@ struct PrimeRun {
                 pointwise(t, rg.x);
                 inv_pass<PASS>(t, rg.x);
             }
-            to_smem<PASS>(t, rg.x);
+            to_smem<PASS, PASS == 1 && NP == 2>(t, rg.x);  // the inverse's pass 1 only when it is the last
         });
         if constexpr (PASS + 1 < NP) fwd_chain<PASS + 1>();
     }
     template <int PASS>
     CF_HD void inv_chain() {  // inverse passes PASS .. 0 (entry: data in smem in layout PASS + 1)
-        ex.sync();
+        pass_sync<PASS, false>();
         ex.each([&](int t, Regs<G>& rg) CF_INL {
             from_smem<PASS>(t, rg.x);
             inv_pass<PASS>(t, rg.x);
-            if (PASS > 0) to_smem<PASS>(t, rg.x);
+            if (PASS > 0) to_smem<PASS, PASS == 1>(t, rg.x);
         });
         if constexpr (PASS > 0) inv_chain<PASS - 1>();
     }
     // spectrum pairs of chunk C (entries 4C .. 4C+3) from tensor memory, then the next chunk
-    template <int C>
+    template <int CH>
     CF_HD void tm_pointwise(int t, u32 ta, u64 (&x)[E], u32 (&b0)[16], u32 (&b1)[16]) const {
-        if constexpr (C < E / 4) {
-            u32(&cur)[16] = (C & 1) ? b1 : b0;
-            u32(&nxt)[16] = (C & 1) ? b0 : b1;
-            if constexpr (C + 1 < E / 4) ex.tmem_ld16(t, ta + 16 * (C + 1), nxt);
+        if constexpr (CH < E / 4) {
+            u32(&cur)[16] = (CH & 1) ? b1 : b0;
+            u32(&nxt)[16] = (CH & 1) ? b0 : b1;
+            if constexpr (CH + 1 < E / 4) ex.tmem_ld16(t, ta + 16 * (CH + 1), nxt);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const u64 w = (u64)cur[4 * k] | ((u64)cur[4 * k + 1] << 32), wq = (u64)cur[4 * k + 2] | ((u64)cur[4 * k + 3] << 32);
-                x[4 * C + k] = shoup_mul_lazy(x[4 * C + k], w, wq, P);
-                if constexpr (W) x[4 * C + k] = red2(x[4 * C + k], 2 * P);
+                x[4 * CH + k] = shoup_mul_lazy(x[4 * CH + k], w, wq, P);
+                if constexpr (W) x[4 * CH + k] = red2(x[4 * CH + k], 2 * P);
             }
             ex.tmem_wait_ld();
-            tm_pointwise<C + 1>(t, ta, x, b0, b1);
+            tm_pointwise<CH + 1>(t, ta, x, b0, b1);
         }
     }
     CF_HD void pointwise(int t, u64 (&x)[E]) const {
         if constexpr (TM) {
-            const u32 ta = X::tmem_addr((u32)misc()[MI_TMEM], t);
+            const u32 ta = X::tmem_addr((u32)misc()[MI_TMEM], lt(t));
             u32 b0[16], b1[16];
             ex.tmem_ld16(t, ta, b0);
             ex.tmem_wait_ld();
@@ -619,7 +699,7 @@ struct PrimeRun {
     // kernel spectrum
     template <int PASS>
     CF_HD void fwd_only_chain() {
-        ex.sync();
+        pass_sync<PASS, true>();
         ex.each([&](int t, Regs<G>& rg) CF_INL {
             from_smem<PASS>(t, rg.x);
             fwd_pass<PASS>(t, rg.x);
@@ -639,13 +719,13 @@ struct PrimeRun {
         }
     }
 
-    // Block sum mod p of the values the threads left in RED[t] (returned to every thread).
+    // Block sum mod p of the values the CTA's threads left in RED[t] (returned to every thread).
     CF_HD u64 sum_red() {
         u64* red = sm + Smem<G>::RED;
         ex.sync();
-        ex.reduce_mod(red, T, P);
+        ex.reduce_mod(red, CT, P);
         ex.sync();
-        return red[T];
+        return red[CT];
     }
 
     // value of a pair table, canonical
@@ -665,28 +745,32 @@ struct PrimeRun {
     // go to six warps, fewer warps looping over them; a group's lanes raise a common base (h, h^TA
     // or h^T, which every lane squares up itself) to their own small exponent, so the deepest chain
     // is about 20 products, and h comes from the table of g(v) built at setup.  The other warps go
-    // straight on with stage 1: the tables are read only after its barriers.
-    static constexpr int TA = T < 32 ? T : 32, TB = T / TA;
-    static constexpr int LW = T < 32 ? T : 32;  // lanes of a warp
+    // straight on with stage 1: the tables are read only after its barriers.  In a cluster, t is the
+    // thread's index in its CTA and J[j] = h^(c CT + T j) carries the CTA's offset c CT.
+    static constexpr int TA = CT < 32 ? CT : 32, TB = CT / TA;
+    static constexpr int LW = CT < 32 ? CT : 32;  // lanes of a warp
     CF_HD static constexpr int log2c(int x) { return x <= 1 ? 0 : 1 + log2c(x / 2); }
     CF_HD void power_tables(int v) {
         u64* pw = sm + Smem<G>::PW;
         const u64* gm = Gm();
         ex.each([&](int t, Regs<G>&) CF_INL {
             const int lane = t & 31;
-            for (int gi = t >> 5; gi < 6; gi += NW) {
+            for (int gi = lt(t) >> 5; gi < 6; gi += NW) {
                 const int base = gi & 1, kind = gi >> 1;
                 const int size = kind == 0 ? TA : kind == 1 ? TB : E + 2;
                 if (lane >= size) continue;
                 const Mod m = md();
                 u64* tab = pw + base * Smem<G>::PW_STRIDE;
                 u64 b = CF_LDG(gm + 2 * v + 1 - base);  // 1/g(v) or g(v)
+                u64 off = m.r1;                          // h^(c CT): the CTA's offset (clusters)
+                if constexpr (C > 1)
+                    if (kind == 2 && rank() > 0) off = mont_pow(b, (u64)rank() * CT, m);
                 const int sq = kind == 0 ? 0 : kind == 1 ? log2c(TA) : log2c(T);
                 for (int i = 0; i < sq; ++i) b = mont_mul(b, b, m);
                 for (int k = lane; k < size; k += LW) {
                     if (kind == 0) tab[PW_A + k] = mont_pow(b, (u64)k, m);
                     else if (kind == 1) tab[PW_B + k] = mont_pow(b, (u64)k, m);
-                    else if (k < E) tab[PW_J + k] = mont_pow(b, (u64)k, m);
+                    else if (k < E) tab[PW_J + k] = C > 1 ? mont_mul(mont_pow(b, (u64)k, m), off, m) : mont_pow(b, (u64)k, m);
                     else if (k == E) {
                         const u64 y = from_mont(mont_pow(b, (u64)NCH, m), m);
                         tab[PW_STEP] = y;
@@ -708,7 +792,8 @@ struct PrimeRun {
     // j >= j0 with j = c (mod NCH), from A[t % TA] B[t / TA] J[j].
     CF_HD void power_chains(int base, int t, const Mod& m, u64 (&f)[NCH], u64& step, u64& stepq, int j0 = 0) const {
         const u64* pw = sm + Smem<G>::PW + base * Smem<G>::PW_STRIDE;
-        const u64 ab = TB > 1 ? mont_mul(pw[PW_A + t % TA], pw[PW_B + t / TA], m) : pw[PW_A + t];
+        const int tl = lt(t);
+        const u64 ab = TB > 1 ? mont_mul(pw[PW_A + tl % TA], pw[PW_B + tl / TA], m) : pw[PW_A + tl];
 #pragma unroll
         for (int c = 0; c < NCH; ++c) {
             const int jc = j0 + ((c - j0) & (NCH - 1));
@@ -733,7 +818,7 @@ struct PrimeRun {
     // work of fast/cuckoo_fast.cu:797-839, done on the device).
     // ---------------------------------------------------------------------------------------
     CF_HD void setup() {
-        u64* red = sm + Smem<G>::RED;  // red[t]: prefix before chunk t; red[T + t]: chunk product / suffix
+        u64* red = sm + Smem<G>::RED;  // red[t]: prefix before chunk t; red[CT + t]: chunk product / suffix
         u64* mi = misc();
         const int F = kp.F, n = kp.n, J = kp.J;
         ex.single([&]() CF_INL {
@@ -743,76 +828,83 @@ struct PrimeRun {
             mi[MI_R1Q] = shoup_companion(m.r1, P);
         });
         ex.sync();
-        const int C = (F + 1 + T - 1) / T;  // factorial entries k = 0..F, chunk of C per thread
-        // product of the integers in each chunk (Montgomery form)
-        ex.each([&](int t, Regs<G>&) CF_INL {
-            const Mod m = md();
-            const int k0 = t * C > 1 ? t * C : 1, k1 = (t + 1) * C < F + 1 ? (t + 1) * C : F + 1;
-            u64 pr = m.r1;
-            u64 km = to_mont((u64)k0, m);
-            for (int k = k0; k < k1; ++k) {
-                pr = mont_mul(pr, km, m);
-                km = madd(km, m.r1, P);
-            }
-            red[T + t] = pr;
-        });
-        ex.sync();
-        ex.single([&]() CF_INL {  // exclusive prefix products, F!, 1/F!, exclusive suffix products / F!
-            const Mod m = md();
-            u64 run = m.r1;
-            for (int t = 0; t < T; ++t) {
-                red[t] = run;
-                run = mont_mul(run, red[T + t], m);
-            }
-            u64 suf = mont_pow(run, P - 2, m);  // 1/F!
-            for (int t = T - 1; t >= 0; --t) {
-                const u64 c = red[T + t];
-                red[T + t] = suf;  // 1/F! times the product of the chunks after t = 1/(last k of chunk t)!
-                suf = mont_mul(suf, c, m);
-            }
-        });
-        ex.sync();
-        ex.each([&](int t, Regs<G>&) CF_INL {
-            const Mod m = md();
-            const int k0 = t * C, k1 = (t + 1) * C < F + 1 ? (t + 1) * C : F + 1;
-            u64 run = red[t];  // (k0 - 1)! (Montgomery), 1 for the first chunk
-            u64 km = to_mont((u64)(k0 > 0 ? k0 : 1), m);
-            for (int k = k0; k < k1; ++k) {  // k! = (k-1)! k
-                if (k > 0) {
-                    run = mont_mul(run, km, m);
+        // The prime's tables in global memory: one CTA builds them (the cluster's first, which its
+        // other CTAs wait for at the cluster barrier below).
+        if (rank() == 0) {
+            const int CH = (F + 1 + CT - 1) / CT;  // factorial entries k = 0..F, chunk of CH per thread
+            // product of the integers in each chunk (Montgomery form)
+            ex.each([&](int t, Regs<G>&) CF_INL {
+                const Mod m = md();
+                const int k0 = t * CH > 1 ? t * CH : 1, k1 = (t + 1) * CH < F + 1 ? (t + 1) * CH : F + 1;
+                u64 pr = m.r1;
+                u64 km = to_mont((u64)k0, m);
+                for (int k = k0; k < k1; ++k) {
+                    pr = mont_mul(pr, km, m);
                     km = madd(km, m.r1, P);
                 }
-                put_pair(fact(), k, from_mont(run, m));
-            }
-            run = red[T + t];  // 1/(k1 - 1)!
-            for (int k = k1 - 1; k >= k0; --k) {  // 1/(k-1)! = k / k!
-                put_pair(ifact(), k, from_mont(run, m));
-                if (k > 0) run = mont_mul(run, to_mont((u64)k, m), m);
-            }
-        });
-        ex.sync();
-        // inv[k] = (k-1)!/k!, D[k] = 1/k!^2, Kq[k] = companion of k; query partial sums zeroed
-        ex.each([&](int t, Regs<G>&) CF_INL {
-            for (int k = t; k <= F; k += T) put_pair(inv(), k, k ? canon(sh(val(ifact(), k), fact(), k - 1)) : 0);
-            for (int k = t; k <= n; k += T) put_pair(D(), k, canon(sh(val(ifact(), k), ifact(), k)));
-            // g(k) and 1/g(k), Montgomery form: C(k, d) and its inverse, or k^d and (1/k)^d
-            const Mod m = md();
-            for (int k = t; k <= n; k += T) {
-                u64 g = 0, gi = 0;
-                if (kp.model == MODEL_REPLACEMENT) {
-                    if (k > 0) {
-                        g = mont_pow(to_mont((u64)k, m), (u64)kp.d, m);
-                        gi = mont_pow(to_mont(inv()[2 * k], m), (u64)kp.d, m);  // this thread wrote inv[k]
-                    }
-                } else if (k >= kp.d) {
-                    g = to_mont(canon(sh(sh(val(fact(), k), ifact(), kp.d), ifact(), k - kp.d)), m);
-                    gi = to_mont(canon(sh(sh(val(ifact(), k), fact(), kp.d), fact(), k - kp.d)), m);
+                red[CT + t] = pr;
+            });
+            ex.sync();
+            ex.single([&]() CF_INL {  // exclusive prefix products, F!, 1/F!, exclusive suffix products / F!
+                const Mod m = md();
+                u64 run = m.r1;
+                for (int t = 0; t < CT; ++t) {
+                    red[t] = run;
+                    run = mont_mul(run, red[CT + t], m);
                 }
-                Gm()[2 * k] = g;
-                Gm()[2 * k + 1] = gi;
-            }
+                u64 suf = mont_pow(run, P - 2, m);  // 1/F!
+                for (int t = CT - 1; t >= 0; --t) {
+                    const u64 c = red[CT + t];
+                    red[CT + t] = suf;  // 1/F! times the product of the chunks after t = 1/(last k of chunk t)!
+                    suf = mont_mul(suf, c, m);
+                }
+            });
+            ex.sync();
+            ex.each([&](int t, Regs<G>&) CF_INL {
+                const Mod m = md();
+                const int k0 = t * CH, k1 = (t + 1) * CH < F + 1 ? (t + 1) * CH : F + 1;
+                u64 run = red[t];  // (k0 - 1)! (Montgomery), 1 for the first chunk
+                u64 km = to_mont((u64)(k0 > 0 ? k0 : 1), m);
+                for (int k = k0; k < k1; ++k) {  // k! = (k-1)! k
+                    if (k > 0) {
+                        run = mont_mul(run, km, m);
+                        km = madd(km, m.r1, P);
+                    }
+                    put_pair(fact(), k, from_mont(run, m));
+                }
+                run = red[CT + t];  // 1/(k1 - 1)!
+                for (int k = k1 - 1; k >= k0; --k) {  // 1/(k-1)! = k / k!
+                    put_pair(ifact(), k, from_mont(run, m));
+                    if (k > 0) run = mont_mul(run, to_mont((u64)k, m), m);
+                }
+            });
+            ex.sync();
+            // inv[k] = (k-1)!/k!, D[k] = 1/k!^2, Kq[k] = companion of k
+            ex.each([&](int t, Regs<G>&) CF_INL {
+                for (int k = t; k <= F; k += CT) put_pair(inv(), k, k ? canon(sh(val(ifact(), k), fact(), k - 1)) : 0);
+                for (int k = t; k <= n; k += CT) put_pair(D(), k, canon(sh(val(ifact(), k), ifact(), k)));
+                // g(k) and 1/g(k), Montgomery form: C(k, d) and its inverse, or k^d and (1/k)^d
+                const Mod m = md();
+                for (int k = t; k <= n; k += CT) {
+                    u64 g = 0, gi = 0;
+                    if (kp.model == MODEL_REPLACEMENT) {
+                        if (k > 0) {
+                            g = mont_pow(to_mont((u64)k, m), (u64)kp.d, m);
+                            gi = mont_pow(to_mont(inv()[2 * k], m), (u64)kp.d, m);  // this thread wrote inv[k]
+                        }
+                    } else if (k >= kp.d) {
+                        g = to_mont(canon(sh(sh(val(fact(), k), ifact(), kp.d), ifact(), k - kp.d)), m);
+                        gi = to_mont(canon(sh(sh(val(ifact(), k), fact(), kp.d), fact(), k - kp.d)), m);
+                    }
+                    Gm()[2 * k] = g;
+                    Gm()[2 * k + 1] = gi;
+                }
+            });
+        }
+        // query partial sums zeroed (each CTA's own)
+        ex.each([&](int t, Regs<G>&) CF_INL {
             const size_t nps = (size_t)J * (n + 1);
-            for (size_t k = t; k < nps; k += T) ps()[k] = 0;
+            for (size_t k = lt(t); k < nps; k += CT) ps()[k] = 0;
         });
         // a root of unity of order L: x^((p-1)/L) whose (L/2)-th power is -1 (fast/cuckoo_fast.cu:815-820)
         ex.single([&]() CF_INL {
@@ -827,30 +919,37 @@ struct PrimeRun {
                     break;
                 }
             }
-            if (!found) ex.set_error(kp.err, KERR_NO_ROOT);
+            if (!found && rank() == 0) ex.set_error(kp.err, KERR_NO_ROOT);
             mi[MI_ROOT] = w;
             mi[MI_LINV] = from_mont(mont_pow(to_mont((u64)L, m), P - 2, m), m);  // 1/L, canonical
         });
         ex.sync();
+        // w^k into every table that holds it: the pass-0 tables by level (global, the first CTA)
+        // and the multiples of 2^R of the later passes (every CTA's shared memory)
         ex.each([&](int t, Regs<G>&) CF_INL {
             const Mod m = md();
             const u64 w = mi[MI_ROOT];
-            u64 cur = mont_pow(w, (u64)t, m);
-            const u64 step = mont_pow(w, (u64)T, m);
-            for (int k = t; k <= L / 2; k += T) {  // w^k into every table that holds it
-                const u64 c = from_mont(cur, m), cq = companion(c);
-                for (int l = 0; l < G::R && (k & ((1 << l) - 1)) == 0; ++l) {
-                    u64* d = WL(l) + 2 * (k >> l);
-                    d[0] = c, d[1] = cq;
-                }
-                if ((k & ((1 << G::R) - 1)) == 0) {
-                    u64* d = tws() + 2 * (k >> G::R);
-                    d[0] = c, d[1] = cq;
+            const int tl = lt(t);
+            u64 cur = mont_pow(w, (u64)tl, m);
+            const u64 step = mont_pow(w, (u64)CT, m);
+            for (int k = tl; k <= L / 2; k += CT) {
+                const bool tw = (k & ((1 << G::R) - 1)) == 0;
+                if (rank() == 0 || tw) {
+                    const u64 c = from_mont(cur, m), cq = companion(c);
+                    if (rank() == 0)
+                        for (int l = 0; l < G::R && (k & ((1 << l) - 1)) == 0; ++l) {
+                            u64* d = WL(l) + 2 * (k >> l);
+                            d[0] = c, d[1] = cq;
+                        }
+                    if (tw) {
+                        u64* d = tws() + 2 * (k >> G::R);
+                        d[0] = c, d[1] = cq;
+                    }
                 }
                 cur = mont_mul(cur, step, m);
             }
         });
-        ex.sync();
+        csync();  // the first CTA's tables are read below and by every later step
         // kernel spectrum: hat = DIF(ker) / L with ker[t] = 1/t for 1 <= t <= n-1 (fast/cuckoo_fast.cu:829,838-839)
         ex.each([&](int t, Regs<G>& rg) CF_INL {
 #pragma unroll
@@ -875,7 +974,7 @@ struct PrimeRun {
             const u64 linv = mi[MI_LINV];
             const u64 linvq = companion(linv);
             if constexpr (TM) {
-                const u32 ta = X::tmem_addr((u32)mi[MI_TMEM], t);
+                const u32 ta = X::tmem_addr((u32)mi[MI_TMEM], lt(t));
 #pragma unroll
                 for (int c = 0; c < E / 4; ++c) {
                     u32 v[16];
@@ -892,7 +991,7 @@ struct PrimeRun {
                 for (int j = 0; j < E; ++j) put_pair(hat(), G::idx(NP - 1, t, j), canon(shoup_mul_lazy(rg.x[j], linv, linvq, P)));
             }
         });
-        ex.sync();
+        csync();  // no CTA's transform exchange may start while another still reads its spectrum pass
     }
 
     // Row r of V or S into the registers (layout 0): the slot of index i gets entry i of the row
@@ -955,7 +1054,7 @@ struct PrimeRun {
                     c0 = c1, q0 = q1;
                 }
                 const u64 part = canon(shoup_mul_lazy(acc, 1, misc()[MI_ONEQ], P));
-                ex.warp_sum_store(t, part, P, qs + (size_t)jq * NW, 1);
+                ex.warp_sum_store(lt(t), part, P, qs + (size_t)jq * NW, 1);
             });
         }
     }
@@ -964,11 +1063,11 @@ struct PrimeRun {
     CF_HD void fold_queries(int q) {
         const u64* qs = sm + Smem<G>::QS;
         ex.each([&](int t, Regs<G>&) CF_INL {
-            const int w = t >> 5, lane = t & 31;
+            const int w = lt(t) >> 5, lane = t & 31;
             for (int jq = w; jq < kp.J; jq += NW) {
                 if (kp.qn[jq] < q) continue;
                 const u64 v = lane < NW ? qs[(size_t)jq * NW + lane] : 0;
-                ex.warp_sum_store(t, v, P, ps() + (size_t)jq * (kp.n + 1) + q, 0);
+                ex.warp_sum_store(lt(t), v, P, ps() + (size_t)jq * (kp.n + 1) + q, 0);
             }
         });
     }
@@ -1012,7 +1111,7 @@ struct PrimeRun {
             fold_queries(v);  // after the transform's barriers: every warp's partial of row v is in
         }
         if (v >= d0) {  // stage 2: column v of V from row v of S
-            ex.sync();  // column v of S is read below
+            csync();  // column v of S is read below
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const Mod m = md();
                 u64 f[NCH], step, stepq;  // g^-(t + jT)
@@ -1106,7 +1205,7 @@ struct PrimeRun {
         }
         const int v0 = tile_v0(v);
         if (v - v0 == TILE - 1 || v == n - 1) {  // move the tile's columns v0 .. v into the rows
-            ex.sync();
+            csync();
             // Rows of later groups only: a row of this tile's group reads these columns from the tile.
             // A full tile goes out in whole 32-byte sectors (4 columns of a block row).
             ex.each([&](int t, Regs<G>&) CF_INL {
@@ -1142,7 +1241,7 @@ struct PrimeRun {
             });
             if (kp.keep) keep_tile(v0, v);
         }
-        ex.sync();  // row v + 1 is read by the next step
+        csync();  // row v + 1 is read by the next step
     }
 
     // Serving builds: the tile's columns v0 .. v of V, for every row below them, into the resident
@@ -1173,31 +1272,34 @@ struct PrimeRun {
             ex.sync();
             fold_queries(n);
         }
-        ex.sync();
-        for (int jq = 0; jq < kp.J; ++jq) {
-            const int nj = kp.qn[jq], Mj = kp.qM[jq];
-            ex.each([&](int t, Regs<G>&) CF_INL {
-                const Mod m = md();
-                u64 Qm;
-                if (kp.model == MODEL_REPLACEMENT) Qm = mont_pow(to_mont((u64)Mj, m), (u64)kp.d, m);
-                else Qm = to_mont(canon(sh(sh(val(fact(), Mj), ifact(), kp.d), ifact(), Mj - kp.d)), m);
-                const u64* pst = ps() + (size_t)jq * (n + 1);
-                u64 acc = 0;
-                for (int k = t + 1; k <= nj; k += T) {
-                    u64 y = pst[k];
-                    y = sh(y, inv(), k);
-                    y = sh(y, ifact(), nj - k);
-                    y = sh(y, ifact(), Mj - k);
-                    if constexpr (W) y = canon(y);  // a factor below 2^62 keeps mont_mul exact
-                    y = mont_mul(y, mont_pow(Qm, (u64)(nj - k), m), m);
-                    acc = madd(acc, y, P);
-                }
-                red[t] = acc;
-            });
-            const u64 s = sum_red();
-            ex.single([&]() CF_INL {
-                kp.out[kp.qout ? (size_t)kp.qout[jq] : (size_t)b * kp.J + jq] = canon(sh(canon(sh(s, fact(), nj)), fact(), Mj));
-            });
+        csync();  // every CTA's row sums are in
+        if (rank() == 0) {  // in a cluster, the first CTA adds up the CTAs' row sums
+            for (int jq = 0; jq < kp.J; ++jq) {
+                const int nj = kp.qn[jq], Mj = kp.qM[jq];
+                ex.each([&](int t, Regs<G>&) CF_INL {
+                    const Mod m = md();
+                    u64 Qm;
+                    if (kp.model == MODEL_REPLACEMENT) Qm = mont_pow(to_mont((u64)Mj, m), (u64)kp.d, m);
+                    else Qm = to_mont(canon(sh(sh(val(fact(), Mj), ifact(), kp.d), ifact(), Mj - kp.d)), m);
+                    const size_t pj = (size_t)jq * (n + 1);
+                    u64 acc = 0;
+                    for (int k = t + 1; k <= nj; k += CT) {
+                        u64 y = ps_of(0)[pj + k];
+                        for (int c = 1; c < C; ++c) y = madd(y, ps_of(c)[pj + k], P);
+                        y = sh(y, inv(), k);
+                        y = sh(y, ifact(), nj - k);
+                        y = sh(y, ifact(), Mj - k);
+                        if constexpr (W) y = canon(y);  // a factor below 2^62 keeps mont_mul exact
+                        y = mont_mul(y, mont_pow(Qm, (u64)(nj - k), m), m);
+                        acc = madd(acc, y, P);
+                    }
+                    red[t] = acc;
+                });
+                const u64 s = sum_red();
+                ex.single([&]() CF_INL {
+                    kp.out[kp.qout ? (size_t)kp.qout[jq] : (size_t)b * kp.J + jq] = canon(sh(canon(sh(s, fact(), nj)), fact(), Mj));
+                });
+            }
         }
     }
 

@@ -69,6 +69,8 @@ def lib():
         L.cf_tables_query_async.restype = ctypes.c_int
         L.cf_engine_set_max_ctas.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.cf_engine_set_max_ctas.restype = ctypes.c_int
+        L.cf_engine_set_transform_lg.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.cf_engine_set_transform_lg.restype = ctypes.c_int
         L.cf_tune_variants.argtypes = [ctypes.c_int, _intp, _intp, _intp, ctypes.c_int]
         L.cf_tune_variants.restype = ctypes.c_int
         L.cf_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -262,6 +264,10 @@ class Engine:
 
     def tune_get(self, lg):
         return int(lib().cf_tune_get(self._h, lg))
+
+    def set_transform_lg(self, lg):
+        """Transforms of at least 2^lg entries (0: the reference's length); residues do not change."""
+        self._check(lib().cf_engine_set_transform_lg(self._h, lg))
 
     def set_max_ctas(self, n):
         """At most n primes (CTAs) per launch of this engine's batches (0: no cap)."""

@@ -71,8 +71,11 @@ const char* cf_engine_last_error(const cf_engine* e);
  * the J queries (qn[j], qM[j]); residues[b*J + j] = N_bad(qn[j], qM[j]) mod primes[b].
  * Replaces the body of the batch loop, fast/cuckoo_fast.cu:787-901: per-prime tables (:797-839),
  * the step loop (:841-855), k_query (:867-876) and the Horner finish (:877-890).
- * Requirements: 1 <= qn[j] <= nmax, qM[j] > qn[j], d <= qM[j] for the subset model, every prime
- * odd, < 2^50, > max(nmax, qM), with transform_length(nmax) dividing p - 1.
+ * Requirements: 1 <= qn[j] <= nmax <= 65536, qM[j] > qn[j], d <= qM[j] for the subset model, every
+ * prime odd, < 2^62 (< 2^50 when nmax > 16384), > max(nmax, qM), with transform_length(nmax)
+ * dividing p - 1.  Tables up to nmax = 16384 take one CTA per prime; larger ones a thread-block
+ * cluster of 4 to 16 CTAs per prime (the reference runs up to nmax < 2^20, :61, :692, with all of
+ * a GPU's threads on a batch of primes).
  * Host buffers; returns when the residues are in `residues`. */
 int cf_residues(cf_engine* e, const uint64_t* primes, int B, int nmax, int d, int model, const int* qn, const int* qM,
                 int J, uint64_t* residues);
@@ -123,7 +126,12 @@ void cf_batch_graph_destroy(cf_batch_graph* g);
  * Mmax), d) through cf_residues, checks that all give the same residues, and makes the fastest
  * the engine's choice for that length (rates[i]: primes per second of geometry i, *chosen: the
  * index).  cf_tune_set / cf_tune_get pin or read the choice (e.g. from a cache of earlier runs).
- * Primes below 2^62 always use the default geometry. */
+ * Primes below 2^62 always use the default geometry.
+ * Transform lengths 2^15 and 2^16 (nmax > 16384) run one prime per thread-block cluster: their
+ * variants are the cluster sizes compiled (smaller first; threads = CTA size, 16 entries each, one
+ * CTA per SM).  By default a launch takes the size with the fewest waves of resident clusters per
+ * CTA of a prime; cf_tune_set(e, lg, i) pins variant i, -1 goes back to that choice, and cf_tune_get
+ * returns the pinned index or -1.  cf_autotune does not time them. */
 int cf_tune_variants(int lg, int* log2_entries, int* threads, int* ctas_per_sm, int cap);
 int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, int cap, int* chosen);
 int cf_tune_set(cf_engine* e, int lg, int variant);
@@ -164,6 +172,13 @@ int cf_tables_query_async(cf_engine* e, const cf_tables* t, const int* qn, const
 /* At most n primes (CTAs) per launch for this engine's batches (0: no cap), so a long batch leaves
  * SMs to work on other streams. */
 int cf_engine_set_max_ctas(cf_engine* e, int n);
+
+/* Transforms of at least 2^lg entries for this engine's batches (0, the default: the reference's
+ * transform_length(nmax)).  The convolutions are exact at every length from transform_length(nmax)
+ * up, so the residues do not change; it runs the kernels of long transforms on small tables (tests)
+ * and needs primes with 2^lg | p - 1 (every prime of the fixed lists, whose p - 1 has the factor
+ * 2^20).  No counterpart in the reference, which fixes the length per batch (:460-472). */
+int cf_engine_set_transform_lg(cf_engine* e, int lg);
 
 /* ---- uneven batches: many instances in one graph of work-queue launches ----
  * Instances k = 0 .. K-1, (n[k], M[k], d[k]) under one model and prime list (bits = 50 or 62):

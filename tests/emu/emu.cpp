@@ -2,9 +2,13 @@
 // cuckoo-failure_b200/csrc/suffix_engine.cuh on the CPU, one emulated thread after another between
 // barriers, so the index logic of the CUDA kernel can be checked against the oracle without a GPU.
 // It is never linked into the product library and is not a fallback for it.
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
+#include <string>
+#include <thread>
 #include <vector>
 
 // every value bound the transforms rely on is checked here (suffix_engine.cuh: check_bound)
@@ -14,13 +18,56 @@
 
 using namespace cfb;
 
+// A cluster's CTAs run as host threads, one per CTA, meeting at the cluster barriers; each CTA's
+// shared memory is its own array, which the others write through st_remote.
+struct ClusterShared {
+    int C = 1;
+    std::vector<u64*> smem;  // each CTA's shared memory
+    size_t words = 0;
+    std::mutex mu;
+    std::condition_variable cv;
+    int arrived = 0;
+    long gen = 0;
+    bool aborted = false;  // a CTA failed: the barriers stop waiting so the others end too
+    void wait() {
+        std::unique_lock<std::mutex> lk(mu);
+        if (aborted) return;
+        const long g = gen;
+        if (++arrived == C) {
+            arrived = 0;
+            ++gen;
+            cv.notify_all();
+        } else {
+            cv.wait(lk, [&] { return gen != g || aborted; });
+        }
+    }
+    void abort() {
+        std::lock_guard<std::mutex> lk(mu);
+        aborted = true;
+        cv.notify_all();
+    }
+};
+
 template <class G>
 struct HostExec {
     std::vector<Regs<G>> regs;
-    HostExec() : regs(G::T) {}
+    int rk = 0;                   // CTA rank in the cluster
+    ClusterShared* cl = nullptr;  // the cluster (null: a lone CTA)
+    u64* own = nullptr;           // this CTA's shared memory
+    HostExec() : regs(G::CT) {}
+    int rank() const { return rk; }
     template <class F>
     void each(F&& f) {
-        for (int t = 0; t < G::T; ++t) f(t, regs[t]);
+        for (int t = 0; t < G::CT; ++t) f(rk * G::CT + t, regs[t]);
+    }
+    void cluster_sync() {
+        if (cl) cl->wait();
+    }
+    void st_remote(u64* p, int r, u64 v) {
+        const ptrdiff_t off = p - own;
+        if (!cl || r < 0 || r >= cl->C || off < 0 || (size_t)off >= cl->words)
+            throw std::runtime_error("distributed shared memory store out of range");
+        cl->smem[r][off] = v;
     }
     template <class F>
     void single(F&& f) {
@@ -41,7 +88,9 @@ struct HostExec {
     }
     u32* tmem_word(int t, u32 ta, int k) {
         const int lane = (int)(ta >> 16) + (t & 31), col = (int)(ta & 0xFFFF) + k;
-        if (lane >= 128 || col >= 512) throw std::runtime_error("tensor memory address out of range");
+        // the columns the device allocates: all 512, or 4 E CT / 128 (at least 32) for a cluster's CTA
+        const int cols = G::C == 1 ? 512 : (4 * G::E * (G::CT / 128) < 32 ? 32 : 4 * G::E * (G::CT / 128));
+        if (lane >= 128 || col >= cols) throw std::runtime_error("tensor memory address out of range");
         return &tm[(size_t)lane * 512 + col];
     }
     void tmem_st16(int t, u32 ta, const u32 (&v)[16]) {
@@ -64,6 +113,38 @@ struct HostExec {
         red[T] = s;
     }
 };
+
+// The cluster kernel (transform length 2^LG on 2^LC CTAs per prime, 16 entries per thread).
+template <int LG, int LC>
+static int run_cluster(const KParams& kp) {
+    typedef Geo<LG, 4, LC> G;
+    const size_t words = Smem<G>::bytes_for(kp.J) / 8;
+    for (int b = 0; b < kp.B; ++b) {
+        ClusterShared cs;
+        cs.C = G::C;
+        cs.words = words;
+        std::vector<std::vector<u64>> sm(G::C, std::vector<u64>(words, 0xA5A5A5A5A5A5A5A5ull));
+        for (int c = 0; c < G::C; ++c) cs.smem.push_back(sm[c].data());
+        std::vector<std::string> errs(G::C);
+        std::vector<std::thread> th;
+        for (int c = 0; c < G::C; ++c)
+            th.emplace_back([&, c] {
+                try {
+                    HostExec<G> ex;
+                    ex.rk = c, ex.cl = &cs, ex.own = sm[c].data();
+                    PrimeRun<G, HostExec<G>, false> pr(ex, kp, b, sm[c].data());
+                    pr.run();
+                } catch (const std::exception& e) {
+                    errs[c] = e.what();
+                    cs.abort();
+                }
+            });
+        for (std::thread& x : th) x.join();
+        for (const std::string& e : errs)
+            if (!e.empty()) throw std::runtime_error(e);
+    }
+    return 0;
+}
 
 template <int LG>
 struct RFor {
@@ -260,6 +341,32 @@ extern "C" int emu_residues_geo(const uint64_t* primes, int B, int nmax, int d, 
         else if (lg == 12 && R == 3) run_geo<12, 3>(kp);
         else if (lg == 12 && R == 5) run_geo<12, 5>(kp);
         else if (lg == 13 && R == 5) run_geo<13, 5>(kp);
+        else return -4;
+    } catch (const std::runtime_error&) {
+        return -6;
+    }
+    return err ? -5 : 0;
+}
+// The cluster kernels on a table of any size (the transform length forced to 2^lg, as
+// cf_engine_set_transform_lg does): lg = 15 with C = 4 or 8, lg = 16 with C = 8 or 16.
+extern "C" int emu_residues_cluster(const uint64_t* primes, int B, int nmax, int d, int model, const int* qn,
+                                    const int* qM, int J, uint64_t* out, int lg, int C) {
+    int F = nmax;
+    for (int j = 0; j < J; ++j) F = qM[j] > F ? qM[j] : F;
+    if (model == MODEL_SUBSET && d > F) F = d;
+    if ((1ull << lg) < cfh::transform_length((uint64_t)nmax)) return -1;
+    const Layout lo = make_layout(nmax, F, 1 << lg, J, 1, 4, 16);  // row sums for the largest cluster, as the engine lays out
+    std::vector<u64> ws(lo.total * (size_t)B, 0xA5A5A5A5A5A5A5A5ull);
+    int err = 0;
+    KParams kp;
+    kp.primes = primes, kp.B = B, kp.n = nmax, kp.F = F, kp.d = d, kp.d0 = model == MODEL_SUBSET ? d : 1;
+    kp.model = model, kp.J = J, kp.qn = qn, kp.qM = qM, kp.ws = ws.data(), kp.ws_words = lo.total, kp.lay = lo;
+    kp.out = out, kp.err = &err;
+    try {
+        if (lg == 15 && C == 4) run_cluster<15, 2>(kp);
+        else if (lg == 15 && C == 8) run_cluster<15, 3>(kp);
+        else if (lg == 16 && C == 8) run_cluster<16, 3>(kp);
+        else if (lg == 16 && C == 16) run_cluster<16, 4>(kp);
         else return -4;
     } catch (const std::runtime_error&) {
         return -6;

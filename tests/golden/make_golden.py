@@ -9,9 +9,11 @@ oracle/Makefile.ref into oracle/_ref/: the 64-bit batch engine's host build
 Run from the repository root, where the reference tree is available:
     make -f oracle/Makefile.ref && python tests/golden/make_golden.py [--groups base,large]
 
-Groups: `base` (small sizes, config 2, one or two primes at n = 16384, the library CLI at small n)
-and `large` (the replacement model at n = 4096 and 16384 through the library's --mod P, 18 queries
-at n <= 16384, and a seeded sample of the uneven-batch workload).
+Groups: `base` (small sizes, config 2, one or two primes at n = 16384, the library CLI at small n),
+`large` (the replacement model at n = 4096 and 16384 through the library's --mod P, 18 queries
+at n <= 16384, and a seeded sample of the uneven-batch workload) and `huge` (tables above
+n = 16384: n = 32768 and n = 65536, primes 0 and 1, one host-build process per prime; the
+n = 65536 runs take 32 GB of host memory each and run one after the other).
 """
 import argparse
 import concurrent.futures as cf
@@ -118,10 +120,27 @@ def large():
     print("large fixtures written")
 
 
+def huge():
+    """Tables above n = 16384 (transform lengths 2^15 and 2^16), d = 3, primes 0 and 1."""
+    for n, queries, parallel in ((32768, [(32768, 65536), (20000, 50000)], True), (65536, [(65536, 131072)], False)):
+        if parallel:
+            with cf.ThreadPoolExecutor(2) as ex:
+                outs = list(ex.map(lambda i: fast_lines(3, queries, i, 1), (0, 1)))
+        else:
+            outs = [fast_lines(3, queries, i, 1) for i in (0, 1)]
+        name = f"fast_n{n}_d3.txt"
+        with open(os.path.join(HERE, name), "w") as g:
+            g.write(f"# d=3 queries={' '.join(f'{a},{b}' for a, b in queries)} first=0 count=2 (one run per prime)\n")
+            g.write("".join(outs))
+        print(name, sum(len(o.splitlines()) for o in outs), "lines")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--groups", default="base,large")
     groups = ap.parse_args().groups.split(",")
+    if "huge" in groups:
+        huge()
     if "large" in groups:
         large()
     if "base" not in groups:

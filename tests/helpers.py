@@ -22,7 +22,7 @@ def build_test_libs():
     csrc = os.path.join(ROOT, "cuckoo-failure_b200", "csrc")
     newest = max(os.path.getmtime(os.path.join(csrc, f)) for f in os.listdir(csrc))
     if not os.path.exists(EMU_SO) or os.path.getmtime(EMU_SO) < max(newest, os.path.getmtime(EMU_SRC)):
-        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", EMU_SRC, "-o", EMU_SO], check=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", EMU_SRC, "-o", EMU_SO], check=True)
 
 
 _oracle = None

@@ -101,3 +101,34 @@ def test_emulated_tuning_geometries(nmax, R):
     out = (ctypes.c_uint64 * J)()
     assert L.emu_residues_geo(pr, 1, nmax, 3, 0, qn, qM, J, out, R) == 0
     assert [int(x) for x in out] == h.oracle_residues(P0, nmax, 3, qs)
+
+
+def emu_cluster(primes, nmax, d, queries, lg, C, model=0):
+    """The cluster kernel (transform length 2^lg on C CTAs per prime, run as C host threads that
+    meet at the cluster barriers and write each other's shared memory) on a table of nmax."""
+    import ctypes
+
+    L = h.emu()
+    u64, ci = ctypes.c_uint64, ctypes.c_int
+    L.emu_residues_cluster.argtypes = [ctypes.POINTER(u64), ci, ci, ci, ci, ctypes.POINTER(ci), ctypes.POINTER(ci), ci,
+                                       ctypes.POINTER(u64), ci, ci]
+    L.emu_residues_cluster.restype = ci
+    B, J = len(primes), len(queries)
+    out = (u64 * (B * J))()
+    rc = L.emu_residues_cluster((u64 * B)(*primes), B, nmax, d, model, (ci * J)(*[n for n, _ in queries]),
+                                (ci * J)(*[M for _, M in queries]), J, out, lg, C)
+    assert rc == 0, rc
+    return [[int(x) for x in out[b * J:(b + 1) * J]] for b in range(B)]
+
+
+@pytest.mark.parametrize("lg,C", [(15, 4), (15, 8), (16, 8), (16, 16)])
+@pytest.mark.parametrize("model", [0, 1])
+def test_emulated_cluster_kernel_matches_oracle(lg, C, model):
+    """Tables above n = 16384 run one prime per cluster of CTAs: pass 0 of each transform on every
+    CTA's columns, the exchange through distributed shared memory (with the lazy reduction of the
+    forward values the 2^15 and 2^16 bounds need, checked here), the per-CTA powers, row sums and
+    flushes, and the first CTA's Horner finish over all CTAs' row sums.  Small tables on the long
+    transforms: the residues do not depend on the length."""
+    ps = h.oracle_primes(0, 2)
+    nmax, d, qs = (70, 3, [(70, 150), (33, 71), (5, 9)]) if model == 0 else (40, 2, [(40, 90), (17, 20)])
+    assert emu_cluster(ps, nmax, d, qs, lg, C, model) == [h.oracle_residues(p, nmax, d, qs, model) for p in ps]
