@@ -89,6 +89,44 @@ CF_HD void pin(u64&) {}
 CF_HD void pin_int(int&) {}
 CF_HD void ld_pair(const u64* p, u64& a, u64& b) { a = p[0], b = p[1]; }
 #endif
+// Loads of data a kernel writes itself.  A CTA alone reads its own writes through L1 and the
+// read-only path.  In a cluster (CG), data another CTA wrote in this launch is read from L2 (.cg),
+// where the writer's release at the cluster barrier has made it visible; L1 lines of an earlier
+// read (block cells and tiles are reused) and the read-only path would not see the new values.
+template <bool CG>
+CF_HD void ldp(const u64* p, u64& a, u64& b) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (CG)
+        asm volatile("ld.global.cg.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;" : "=l"(a), "=l"(b) : "l"(p), "l"(policy_keep()));
+    else ld_pair(p, a, b);
+#else
+    a = p[0], b = p[1];
+#endif
+}
+template <bool CG>
+CF_HD u64 lds(const u64* p) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (CG) {
+        u64 v;
+        asm volatile("ld.global.cg.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(policy_stream()));
+        return v;
+    } else return ld_stream(p);
+#else
+    return *p;
+#endif
+}
+template <bool CG>
+CF_HD u64 ldc(const u64* p) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (CG) {
+        u64 v;
+        asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(v) : "l"(p));
+        return v;
+    } else return CF_LDG(p);
+#else
+    return *p;
+#endif
+}
 // Lambdas that index the register array must be inlined, or the array goes to local memory.
 #define CF_INL __attribute__((always_inline))
 // Compile-time slot index handed to the bodies below (so register-array indices are constants).
@@ -114,36 +152,36 @@ CF_HD void window(B&& body, Dn&& done) {
     window_step<N, K, 0>(body, done);
 }
 // Per-slot constant pairs over a window: slot J's pair addr(IC<J>) is loaded D slots ahead.
-template <int N, int D, int K, class A, class F, class Dn>
+template <int N, int D, int K, bool CG = false, class A, class F, class Dn>
 CF_HD void pipe_pairs(A&& addr, F&& apply, Dn&& done) {
     u64 ra[D + 1], rb[D + 1];
     window<D, 0>([&](auto jc) CF_INL {
         constexpr int j = decltype(jc)::value;
-        if constexpr (j < N) ld_pair(addr(jc), ra[j], rb[j]);
+        if constexpr (j < N) ldp<CG>(addr(jc), ra[j], rb[j]);
     }, [&](auto) CF_INL {});
     window<N, K>(
         [&](auto jc) CF_INL {
             constexpr int j = decltype(jc)::value;
-            if constexpr (j + D < N) ld_pair(addr(IC<j + D>{}), ra[(j + D) % (D + 1)], rb[(j + D) % (D + 1)]);
+            if constexpr (j + D < N) ldp<CG>(addr(IC<j + D>{}), ra[(j + D) % (D + 1)], rb[(j + D) % (D + 1)]);
             apply(jc, ra[j % (D + 1)], rb[j % (D + 1)]);
         },
         done);
 }
 // The same over the slots for which live(IC<J>) holds (a warp-uniform test): the others issue
 // neither their constant load nor their unit.
-template <int N, int D, int K, class Lv, class A, class F, class Dn>
+template <int N, int D, int K, bool CG = false, class Lv, class A, class F, class Dn>
 CF_HD void pipe_pairs_live(Lv&& live, A&& addr, F&& apply, Dn&& done) {
     u64 ra[D + 1] = {}, rb[D + 1] = {};
     window<D, 0>([&](auto jc) CF_INL {
         constexpr int j = decltype(jc)::value;
         if constexpr (j < N)
-            if (live(jc)) ld_pair(addr(jc), ra[j], rb[j]);
+            if (live(jc)) ldp<CG>(addr(jc), ra[j], rb[j]);
     }, [&](auto) CF_INL {});
     window<N, K>(
         [&](auto jc) CF_INL {
             constexpr int j = decltype(jc)::value;
             if constexpr (j + D < N)
-                if (live(IC<j + D>{})) ld_pair(addr(IC<j + D>{}), ra[(j + D) % (D + 1)], rb[(j + D) % (D + 1)]);
+                if (live(IC<j + D>{})) ldp<CG>(addr(IC<j + D>{}), ra[(j + D) % (D + 1)], rb[(j + D) % (D + 1)]);
             if (live(jc)) apply(jc, ra[j % (D + 1)], rb[j % (D + 1)]);
         },
         done);
@@ -359,6 +397,7 @@ template <class G, class X, bool W = false>
 struct PrimeRun {
     static constexpr int L = G::L, T = G::T, E = G::E, NP = G::NP, NW = G::NW;
     static constexpr int C = G::C, CT = G::CT, LCN = G::LCN;  // a cluster of C CTAs of CT threads per prime
+    static constexpr bool CG = C > 1;  // loads of what other CTAs wrote go to L2 (ldp / lds / ldc)
     static_assert(W || G::LG <= 14 || G::FRED, "reduction-free forward transform needs 2^LG p < 2^64");
     static_assert(!W || C == 1, "primes below 2^62 run on one CTA per prime");
     static_assert(NP > 1, "layout 0 must hold index t + jT in slot j of thread t");
@@ -420,7 +459,7 @@ struct PrimeRun {
     }
 
     CF_HD u64 sh(u64 a, const u64* pairs, int k) const {  // a * pairs[k], result in [0, 4p)
-        return shoup_mul_lazy(a, CF_LDG(pairs + 2 * k), CF_LDG(pairs + 2 * k + 1), P);
+        return shoup_mul_lazy(a, ldc<CG>(pairs + 2 * k), ldc<CG>(pairs + 2 * k + 1), P);
     }
     // Shoup companion of w < p, from the per-prime constants setup keeps in shared memory
     CF_HD u64 companion(u64 w) const { return shoup_companion_fast(w, P, misc()[MI_ONEQ], misc()[MI_R1], misc()[MI_R1Q]); }
@@ -492,7 +531,7 @@ struct PrimeRun {
     }
     template <int PASS>
     CF_HD static void ld_tw(const u64* p, u64& a, u64& b) {
-        if constexpr (PASS == 0) ld_pair(p, a, b);
+        if constexpr (PASS == 0) ldp<CG>(p, a, b);
         else ld_pair_shared(p, a, b);
     }
     template <int PASS, bool FWD>
@@ -667,7 +706,7 @@ struct PrimeRun {
             return;
         }
         const u64* h = hat();
-        pipe_pairs<E, PD, WK>(
+        pipe_pairs<E, PD, WK, CG>(
             [&](auto jc) CF_INL { return h + 2 * G::idx(NP - 1, t, decltype(jc)::value); },
             [&](auto jc, u64 w, u64 wq) CF_INL {
                 constexpr int j = decltype(jc)::value;
@@ -729,7 +768,7 @@ struct PrimeRun {
     }
 
     // value of a pair table, canonical
-    CF_HD static u64 val(const u64* pairs, int k) { return CF_LDG(pairs + 2 * k); }
+    CF_HD static u64 val(const u64* pairs, int k) { return ldc<CG>(pairs + 2 * k); }
 
     // The slots' powers h^(t + jT), j = 0 .. E-1, as NCH independent running products: chain c
     // holds h^(t + jT) for j = c (mod NCH) and steps by h^(NCH T), so the products that depend on
@@ -761,7 +800,7 @@ struct PrimeRun {
                 if (lane >= size) continue;
                 const Mod m = md();
                 u64* tab = pw + base * Smem<G>::PW_STRIDE;
-                u64 b = CF_LDG(gm + 2 * v + 1 - base);  // 1/g(v) or g(v)
+                u64 b = ldc<CG>(gm + 2 * v + 1 - base);  // 1/g(v) or g(v)
                 u64 off = m.r1;                          // h^(c CT): the CTA's offset (clusters)
                 if constexpr (C > 1)
                     if (kind == 2 && rank() > 0) off = mont_pow(b, (u64)rank() * CT, m);
@@ -797,7 +836,8 @@ struct PrimeRun {
 #pragma unroll
         for (int c = 0; c < NCH; ++c) {
             const int jc = j0 + ((c - j0) & (NCH - 1));
-            f[c] = jc == 0 ? ab : (jc < E ? mont_mul(ab, pw[PW_J + jc], m) : 0);
+            // J[0] = 1 on a CTA alone; in a cluster it carries the CTA's offset h^(c CT)
+            f[c] = (jc == 0 && C == 1) ? ab : (jc < E ? mont_mul(ab, pw[PW_J + jc], m) : 0);
         }
         step = pw[PW_STEP], stepq = pw[PW_STEPQ];
     }
@@ -810,8 +850,8 @@ struct PrimeRun {
     }
 
     // g(v) and 1/g(v) in Montgomery form, from the table built at setup (0 for v < d0, subset model)
-    CF_HD u64 g_mont(int v) const { return CF_LDG(Gm() + 2 * v); }
-    CF_HD u64 ginv_mont(int v) const { return CF_LDG(Gm() + 2 * v + 1); }
+    CF_HD u64 g_mont(int v) const { return ldc<CG>(Gm() + 2 * v); }
+    CF_HD u64 ginv_mont(int v) const { return ldc<CG>(Gm() + 2 * v + 1); }
 
     // ---------------------------------------------------------------------------------------
     // Setup: factorials, inverses, D, twiddles and the kernel spectrum of 1/t (the per-batch host
@@ -1013,13 +1053,13 @@ struct PrimeRun {
             for (int j = 0; j < E; ++j) {
                 const int i = t + j * T, wg = W0 + j * (T / TILE);  // column group
                 const int cell = wg < h ? wg * a_lo + b_lo : wg * h + b_hi;
-                x[j] = (i >= lo && i < hi) ? ld_stream(i < v0 ? base + ((size_t)cell << 8) : tl + (size_t)(i - v0) * (n + 1)) : 0;
+                x[j] = (i >= lo && i < hi) ? lds<CG>(i < v0 ? base + ((size_t)cell << 8) : tl + (size_t)(i - v0) * (n + 1)) : 0;
             }
         } else {
 #pragma unroll
             for (int j = 0; j < E; ++j) {
                 const int i = G::idx(0, t, j);
-                x[j] = (i >= lo && i < hi) ? ld_stream(i < v0 ? pool + blk_off(r, i, h) : tl + (size_t)(i - v0) * (n + 1)) : 0;
+                x[j] = (i >= lo && i < hi) ? lds<CG>(i < v0 ? pool + blk_off(r, i, h) : tl + (size_t)(i - v0) * (n + 1)) : 0;
             }
         }
     }
@@ -1042,12 +1082,12 @@ struct PrimeRun {
                 const u64* iv = inv() + 2 * (size_t)Mj;  // the pair of 1/(M_j - w) sits at iv - 2w
                 const int tw = t & ~31;                  // the warp's first thread
                 u64 acc = 0, c0 = 0, q0 = 0;
-                if (G::idx(0, t, 0) < q) ld_pair(iv - 2 * G::idx(0, t, 0), c0, q0);
+                if (G::idx(0, t, 0) < q) ldp<CG>(iv - 2 * G::idx(0, t, 0), c0, q0);
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
                     const bool more = j + 1 < E && G::idx(0, tw, j + 1) < q;
                     u64 c1 = 0, q1 = 0;  // slots at or above q multiply by zero
-                    if (more && G::idx(0, t, j + 1) < q) ld_pair(iv - 2 * G::idx(0, t, j + 1), c1, q1);
+                    if (more && G::idx(0, t, j + 1) < q) ldp<CG>(iv - 2 * G::idx(0, t, j + 1), c1, q1);
                     if constexpr (W) acc = madd(acc, canon(shoup_mul_lazy(rg.x[j], c0, q0, P)), P);
                     else acc += shoup_mul_lazy(rg.x[j], c0, q0, P);  // E terms below 4p: < 2^57
                     if (!more) break;
@@ -1083,10 +1123,10 @@ struct PrimeRun {
             query_row(v);
             convolve();
             ex.each([&](int t, Regs<G>& rg) CF_INL {
-                const u64 iv = val(inv(), v), ivq = CF_LDG(inv() + 2 * v + 1);
+                const u64 iv = val(inv(), v), ivq = ldc<CG>(inv() + 2 * v + 1);
                 u64* col = SS() + (size_t)(v - tile_v0(v)) * (n + 1);  // S[.][v], by row
                 const u64* Dt = D();
-                pipe_pairs_live<E, PD, WK>(
+                pipe_pairs_live<E, PD, WK, CG>(
                     [&](auto jc) CF_INL {  // rows v .. n-1 of column v: slots where the warp holds one
                         int lo, hi;
                         warp_slot_range(t, decltype(jc)::value, lo, hi);
@@ -1174,10 +1214,10 @@ struct PrimeRun {
                 const bool wrap0 = n == L && t == 0;  // this thread holds e[n] at index 0
                 if (wrap0 && j0 > 0 && L > v) {
                     u64 c, cq;
-                    ld_pair(Dt + 2 * (L - v - 1), c, cq);
+                    ldp<CG>(Dt + 2 * (L - v - 1), c, cq);
                     st_stream(col + L, entry(rg.x[0], L, c, cq, fwrap, pmL));
                 }
-                pipe_pairs_live<E, PD, WK>(
+                pipe_pairs_live<E, PD, WK, CG>(
                     [&](auto jc) CF_INL {
                         int lo, hi;
                         warp_slot_range(t, decltype(jc)::value, lo, hi);
@@ -1219,11 +1259,11 @@ struct PrimeRun {
                         if (cnt == TILE && v0 > d0) {
 #pragma unroll
                             for (int c = 0; c < TILE; c += 4)
-                                st_stream4(dst + c, ld_stream(src + c * cs), ld_stream(src + (c + 1) * cs),
-                                           ld_stream(src + (c + 2) * cs), ld_stream(src + (c + 3) * cs));
+                                st_stream4(dst + c, lds<CG>(src + c * cs), lds<CG>(src + (c + 1) * cs),
+                                           lds<CG>(src + (c + 2) * cs), lds<CG>(src + (c + 3) * cs));
                         } else {
                             for (int c = 0; c < cnt; ++c)
-                                if (v0 + c > d0) st_stream(dst + c, ld_stream(src + c * cs));
+                                if (v0 + c > d0) st_stream(dst + c, lds<CG>(src + c * cs));
                         }
                     }
                     u64* dst = V() + off;  // row r of V: entries w = v0 .. v, written for w >= d0
@@ -1231,11 +1271,11 @@ struct PrimeRun {
                     if (cnt == TILE && v0 >= d0) {
 #pragma unroll
                         for (int c = 0; c < TILE; c += 4)
-                            st_stream4(dst + c, ld_stream(src + c * cs), ld_stream(src + (c + 1) * cs),
-                                       ld_stream(src + (c + 2) * cs), ld_stream(src + (c + 3) * cs));
+                            st_stream4(dst + c, lds<CG>(src + c * cs), lds<CG>(src + (c + 1) * cs),
+                                       lds<CG>(src + (c + 2) * cs), lds<CG>(src + (c + 3) * cs));
                     } else {
                         for (int c = 0; c < cnt; ++c)
-                            if (v0 + c >= d0) st_stream(dst + c, ld_stream(src + c * cs));
+                            if (v0 + c >= d0) st_stream(dst + c, lds<CG>(src + c * cs));
                     }
                 }
             });
@@ -1255,7 +1295,7 @@ struct PrimeRun {
                 const u64* src = VS() + r;
                 for (int c = 0; c < cnt; ++c) {
                     const int w = v0 + c;
-                    if (w >= d0 && w < r) dst[w] = ld_stream(src + (size_t)c * (n + 1));
+                    if (w >= d0 && w < r) dst[w] = lds<CG>(src + (size_t)c * (n + 1));
                 }
             }
         });
@@ -1284,8 +1324,8 @@ struct PrimeRun {
                     const size_t pj = (size_t)jq * (n + 1);
                     u64 acc = 0;
                     for (int k = t + 1; k <= nj; k += CT) {
-                        u64 y = ps_of(0)[pj + k];
-                        for (int c = 1; c < C; ++c) y = madd(y, ps_of(c)[pj + k], P);
+                        u64 y = ldc<CG>(ps_of(0) + pj + k);
+                        for (int c = 1; c < C; ++c) y = madd(y, ldc<CG>(ps_of(c) + pj + k), P);
                         y = sh(y, inv(), k);
                         y = sh(y, ifact(), nj - k);
                         y = sh(y, ifact(), Mj - k);

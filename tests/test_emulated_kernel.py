@@ -130,5 +130,6 @@ def test_emulated_cluster_kernel_matches_oracle(lg, C, model):
     flushes, and the first CTA's Horner finish over all CTAs' row sums.  Small tables on the long
     transforms: the residues do not depend on the length."""
     ps = h.oracle_primes(0, 2)
-    nmax, d, qs = (70, 3, [(70, 150), (33, 71), (5, 9)]) if model == 0 else (40, 2, [(40, 90), (17, 20)])
+    # rows spread over two or three CTAs (512 or 256 threads each), so every cross-CTA path runs
+    nmax, d, qs = (600, 3, [(600, 1500), (513, 1100), (5, 9)]) if model == 0 else (300, 2, [(300, 700), (17, 20)])
     assert emu_cluster(ps, nmax, d, qs, lg, C, model) == [h.oracle_residues(p, nmax, d, qs, model) for p in ps]

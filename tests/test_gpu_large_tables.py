@@ -20,7 +20,8 @@ CLI = os.path.join(h.ROOT, "cuckoo-failure_b200", "bin", "cuckoo_fast_b200")
 @pytest.mark.parametrize("model", [0, 1])
 def test_cluster_kernels_match_oracle_on_small_tables(lg, variant, model):
     ps = cb.prime_range(0, 3)
-    nmax, d, qs = (300, 3, [(300, 700), (129, 300), (7, 9)]) if model == 0 else (200, 2, [(200, 450), (64, 65)])
+    # rows spread over two or three CTAs of the cluster (512 or 256 threads each)
+    nmax, d, qs = (700, 3, [(700, 1500), (513, 1100), (7, 9)]) if model == 0 else (300, 2, [(300, 700), (64, 65)])
     with cb.Engine(0) as eng:
         eng.set_transform_lg(lg)
         eng.tune_set(lg, variant)

@@ -91,7 +91,7 @@ def test_gpu_rejects_bad_arguments(eng):
         eng.residues([p0], 100, 3, [(100, 100)])  # M must exceed n
     assert e.value.code == cb.CF_ERR_ARG
     with pytest.raises(cb.EngineError) as e:
-        eng.residues([p0], 16385, 3, [(16385, 40000)])
+        eng.residues([p0], 65537, 3, [(65537, 140000)])  # above the largest transform length, 2^16
     assert e.value.code == cb.CF_ERR_UNSUPPORTED
     assert eng.residues([], 100, 3, [(100, 200)]).shape == (0, 1)
 
