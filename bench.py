@@ -31,10 +31,10 @@ sys.path.insert(0, PKG)
 METRIC = "prime-residues/s, n=16384 d=3 NTT suffix build; served-query p50/p99 latency"
 UNIT = "prime-residues/s"
 K_OPS_PER_MM = 20  # INT32 multiply ops per 64-bit modular multiplication (fixed accounting model)
-# DRAM bytes (read + write) per launch of the engine kernel, from the ncu launch list of this
-# bench's own command (profiles/k_suffix_n16384_b148_launches.md), keyed by (n, M, d, primes per
-# launch, prime bits)
-MEASURED_TRAFFIC = {(16384, 32768, 3, 148, 50): 1299.2e9 + 865.1e9}
+# DRAM bytes (read + write) per prime of the engine kernel, from an ncu capture of this bench at 2
+# primes per launch (profiles/k_suffix_n16384_b2_sections.md), keyed by (n, M, d, prime bits); the
+# bench scales it by the primes per launch
+MEASURED_TRAFFIC_PER_PRIME = {(16384, 32768, 3, 50): (4.138317e9 + 4.254311e9) / 2}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 
@@ -173,16 +173,18 @@ def cpu_baseline(n, M, d):
 
 
 def golden_check(n, M, d, bits=50):
-    """Known residues of the reference host build for primes 0 and 1 (tests/golden)."""
-    path = os.path.join(ROOT, "tests", "golden", f"fast{'62' if bits == 62 else ''}_n{n}_d{d}.txt")
-    if not os.path.exists(path):
-        return {}
+    """Known residues of the reference host build (tests/golden): primes 0 and 1, and 0 .. 15 at
+    the headline size."""
     out = {}
-    with open(path) as f:
-        for ln in f:
-            t = ln.split()
-            if len(t) == 5 and not ln.startswith("#") and int(t[2]) == n and int(t[3]) == M:
-                out[int(t[0])] = int(t[4])
+    for suffix in ("", "_first16"):
+        path = os.path.join(ROOT, "tests", "golden", f"fast{'62' if bits == 62 else ''}_n{n}_d{d}{suffix}.txt")
+        if not os.path.exists(path):
+            continue
+        with open(path) as f:
+            for ln in f:
+                t = ln.split()
+                if len(t) == 5 and not ln.startswith("#") and int(t[2]) == n and int(t[3]) == M:
+                    out[int(t[0])] = int(t[4])
     return out
 
 
@@ -382,6 +384,45 @@ def sweep_run(eng, n, M, B, reps=2):
     return out
 
 
+def large_run(device, sizes=((32768, 65536), (65536, 131072)), d=3, reps=1):
+    """Tables above n = 16384 (one prime per thread-block cluster): per size, a wave of as many
+    primes as fit the device (one fewer), one graph-captured launch timed after a warm-up, and one
+    prime alone; residues of primes 0 and 1 checked against the reference host build's.  Beside it
+    the reference's only published timing, at n = 65536 on an H100 (fast/README.md:80-86)."""
+    import numpy as np
+    import torch
+
+    import cuckoo_b200 as cb
+
+    out = {}
+    stream = torch.cuda.Stream()
+    for n, M in sizes:
+        with cb.Engine(device) as eng:
+            B = max(1, eng.max_batch(n, M, 1) - 1)
+            primes = cb.prime_range(0, B)
+            d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
+            d_out = torch.empty(B, dtype=torch.int64, device="cuda")
+            g = eng.batch_graph(d_primes.data_ptr(), B, n, d, [(n, M)], d_out.data_ptr())
+            ms = timed_replays(g.launch, stream, reps)
+            g.status(stream.cuda_stream)
+            g.close()
+            got = d_out.cpu().numpy().view(np.uint64)
+            for i, r in golden_check(n, M, d).items():
+                assert int(got[i]) == r, f"n={n}: residue mismatch at prime {i}"
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record(stream)
+            eng.residues_async(d_primes.data_ptr(), 1, n, d, [(n, M)], d_out.data_ptr(), stream.cuda_stream)
+            q1.record(stream)
+            torch.cuda.synchronize()
+            one = q0.elapsed_time(q1)
+        out[f"n{n}"] = {"value": B / (ms * 1e-3), "unit": UNIT, "primes_per_launch": B, "ms_per_launch": ms,
+                        "one_prime_alone_s": one * 1e-3, "workload": f"n={n}, M={M}, d={d}, one query, 50-bit primes",
+                        "checked": "residues of primes 0 and 1 equal the reference host build's"}
+    out["reference_published"] = ("fast/README.md:80-86: n = 65536, one prime, 126 queries, CUDA batch 2 on an H100: "
+                                  "table build 3.5 s per prime, queries 0.75 s (current version)")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -404,6 +445,7 @@ def main():
     ap.add_argument("--uneven-stride", type=int, default=97)
     ap.add_argument("--no-sweep", action="store_true", help="skip d = 2, 4 and the replacement model")
     ap.add_argument("--no-config2", action="store_true", help="skip the n = 4096 (autotuned) run")
+    ap.add_argument("--no-large", action="store_true", help="skip the tables above n = 16384 (n = 32768, 65536)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="--impl reference: skip the reference's CUDA build (timed beside its host build)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
@@ -543,7 +585,8 @@ def main():
     peak = probe.cfp_imad_ops_per_s(local, 5) / 1e12
     # the timed stream holds only this engine's launches, back to back: per-GPU algorithmic rate
     achieved = B * a.steps * algorithmic_mm(n) * K_OPS_PER_MM / (ms * 1e-3) / 1e12
-    traffic = a.traffic_bytes or MEASURED_TRAFFIC.get((n, M, d, B, a.prime_bits))
+    per_prime = MEASURED_TRAFFIC_PER_PRIME.get((n, M, d, a.prime_bits))
+    traffic = a.traffic_bytes or (per_prime * B if per_prime else None)
     hbm = None
     if traffic:  # the kernel's DRAM bytes per launch (ncu) over its device-timed launch duration
         gbs = traffic / (ms / a.steps * 1e-3) / 1e9
@@ -561,6 +604,9 @@ def main():
         cfg2 = config2_run(local)
         for k in ("default", "tuned"):
             cfg2[k]["frac"] = cfg2[k].pop("frac_top") / peak if peak else None
+    large = None
+    if rank == 0 and world == 1 and not a.no_large:
+        large = large_run(local)
     unev = None
     if rank == 0 and world == 1 and not a.no_uneven:
         with cb.Engine(local) as eng2:
@@ -584,7 +630,8 @@ def main():
                          "model": f"{K_OPS_PER_MM} INT32 multiply ops per modular multiplication, "
                                   f"{algorithmic_mm(n):.3e} multiplications per prime-residue; peak measured live"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-            "plain_form": plain, "config2": cfg2, "config3_sweep": sweep, "uneven": unev, "serving": serving}))
+            "plain_form": plain, "config2": cfg2, "config3_sweep": sweep, "large_tables": large, "uneven": unev,
+            "serving": serving}))
     if dist:
         dist.destroy_process_group()
     return 0

@@ -121,7 +121,13 @@ def large():
 
 
 def huge():
-    """Tables above n = 16384 (transform lengths 2^15 and 2^16), d = 3, primes 0 and 1."""
+    """Tables above n = 16384 (transform lengths 2^15 and 2^16), d = 3, primes 0 and 1; and the
+    headline size n = 16384 for primes 0 .. 15 (one process per prime)."""
+    with cf.ThreadPoolExecutor(max(1, (os.cpu_count() or 2))) as ex:
+        outs = list(ex.map(lambda i: fast_lines(3, [(16384, 32768)], i, 1), range(16)))
+    with open(os.path.join(HERE, "fast_n16384_d3_first16.txt"), "w") as g:
+        g.write("# d=3 queries=16384,32768 first=0 count=16 (one run per prime)\n")
+        g.write("".join(outs))
     for n, queries, parallel in ((32768, [(32768, 65536), (20000, 50000)], True), (65536, [(65536, 131072)], False)):
         if parallel:
             with cf.ThreadPoolExecutor(2) as ex:

@@ -43,7 +43,8 @@ def test_gpu_matches_reference_n4096(eng):
     assert check_golden(eng, "fast_n4096_d3.txt") == 4
 
 
-@pytest.mark.parametrize("name", ["fast_n16384_d2.txt", "fast_n16384_d3.txt", "fast_n16384_d4.txt"])
+@pytest.mark.parametrize("name", ["fast_n16384_d2.txt", "fast_n16384_d3.txt", "fast_n16384_d4.txt",
+                                  "fast_n16384_d3_first16.txt"])
 def test_gpu_matches_reference_n16384(eng, name):
     assert check_golden(eng, name) >= 1
 
