@@ -385,9 +385,9 @@ def sweep_run(eng, n, M, B, reps=2):
 
 
 def large_run(device, sizes=((32768, 65536), (65536, 131072)), d=3, reps=1):
-    """Tables above n = 16384 (one prime per thread-block cluster): per size, a wave of as many
-    primes as fit the device (one fewer), one graph-captured launch timed after a warm-up, and one
-    prime alone; residues of primes 0 and 1 checked against the reference host build's.  Beside it
+    """Tables above n = 16384 (one prime per thread-block cluster): per size, as many primes as fit
+    the device (one fewer), rounded down to whole waves of resident clusters, one graph-captured
+    launch timed after a warm-up, and one prime alone; residues of primes 0 and 1 checked against the reference host build's.  Beside it
     the reference's only published timing, at n = 65536 on an H100 (fast/README.md:80-86)."""
     import numpy as np
     import torch
@@ -398,7 +398,8 @@ def large_run(device, sizes=((32768, 65536), (65536, 131072)), d=3, reps=1):
     stream = torch.cuda.Stream()
     for n, M in sizes:
         with cb.Engine(device) as eng:
-            B = max(1, eng.max_batch(n, M, 1) - 1)
+            fit, wave = max(1, eng.max_batch(n, M, 1) - 1), eng.resident_primes(n, M, 1)
+            B = fit - fit % wave if wave and fit > wave else fit  # whole waves of resident clusters
             primes = cb.prime_range(0, B)
             d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
             d_out = torch.empty(B, dtype=torch.int64, device="cuda")

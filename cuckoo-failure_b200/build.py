@@ -28,10 +28,10 @@ NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xpt
 # Per-unit assembler options.  The L = 2^14 kernel runs 1024 threads, so it has 64 registers per
 # thread; at the default level ptxas schedules its transform passes far past that budget (frames
 # above 800 bytes), while -O1 keeps the 50-bit kernel to a 152-byte frame and the 62-bit one to
-# 320 bytes.  The L = 2^10 kernel is compiled for 16 CTAs per SM (MinBlocks in kernel_lg.cuh), also
+# 320 bytes (the cluster kernel with 1024 threads of 8 entries: 56 bytes).  The L = 2^10 kernel is compiled for 16 CTAs per SM (MinBlocks in kernel_lg.cuh), also
 # 128 registers: -O1 keeps it to a 208-byte frame where the default level spills 1.4 KB.  The other
 # kernels have up to 255 registers and spill at neither level.
-UNIT_FLAGS = {"k_lg14.cu": ["-Xptxas", "-O1"], "k_lg10.cu": ["-Xptxas", "-O1"],
+UNIT_FLAGS = {"k_lg14.cu": ["-Xptxas", "-O1"], "k_lg10.cu": ["-Xptxas", "-O1"], "k_lg15_c4e8.cu": ["-Xptxas", "-O1"],
               "k_lg14_tune.cu": ["-Xptxas", "-O1"], "k_lg10_tune.cu": ["-Xptxas", "-O1"]}
 
 

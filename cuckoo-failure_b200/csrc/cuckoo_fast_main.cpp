@@ -130,7 +130,11 @@ int main(int argc, char** argv) {
         return 1;
     }
     const uint64_t per_prime = cf_workspace_bytes(nmax, Mmax, (int)qs.size());
-    if (batch <= 0) batch = cf_max_batch(eng, nmax, Mmax, (int)qs.size());
+    if (batch <= 0) {  // what fits, rounded down to whole waves of the primes the GPU runs at once
+        batch = cf_max_batch(eng, nmax, Mmax, (int)qs.size());
+        const long wave = cf_resident_primes(eng, nmax, Mmax, (int)qs.size());
+        if (wave > 0 && batch > wave) batch -= batch % wave;
+    }
     if (batch < 1) {
         std::fprintf(stderr, "not enough device memory: %.2f GB per prime\n", per_prime / 1073741824.0);
         cf_engine_destroy(eng);

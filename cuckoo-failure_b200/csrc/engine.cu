@@ -49,9 +49,11 @@ KInfo kernel_for(int lg, bool wide) {
         default: return KInfo{nullptr, 0, 0, 0};
     }
 }
-// The cluster sizes compiled for transform length 2^lg (15, 16), smallest first.
+// The cluster geometries compiled for transform length 2^lg (15, 16): cluster size, and 16 or 8
+// entries per thread (8: twice the threads per CTA); smaller clusters first.
 static int cluster_variants(int lg, KInfo* v) {
-    if (lg == 15) return v[0] = cf_kinfo_lg15_c4(), v[1] = cf_kinfo_lg15_c8(), 2;
+    if (lg == 15)
+        return v[0] = cf_kinfo_lg15_c4(), v[1] = cf_kinfo_lg15_c8(), v[2] = cf_kinfo_lg15_c4_e8(), v[3] = cf_kinfo_lg15_c8_e8(), 4;
     if (lg == 16) return v[0] = cf_kinfo_lg16_c8(), v[1] = cf_kinfo_lg16_c16(), 2;
     return 0;
 }
@@ -71,22 +73,15 @@ static int resident_clusters(const KInfo& ki, size_t smem, cudaStream_t s) {
     if (cudaOccupancyMaxActiveClusters(&n, (const void*)ki.fn, &cfg) != cudaSuccess) return 0;
     return n;
 }
-// The cluster size for a launch of nb primes at transform length 2^lg: the least time per prime,
-// taken as waves (ceil(nb / resident clusters)) over CTAs per prime; ties go to the smaller cluster.
+// The cluster geometry a launch at transform length 2^lg runs: the one pinned on the engine
+// (cf_tune_set, or cf_autotune's choice), else the default, the first of cluster_variants.
 static KInfo pick_cluster(const cf_engine* e, int lg, int nb, int J, cudaStream_t s) {
-    KInfo v[4];
+    (void)nb, (void)J, (void)s;
+    KInfo v[8];
     const int k = cluster_variants(lg, v);
     const int forced = lg > MAX_LG ? e->cluster_pick[lg - MAX_LG - 1] : -1;
     if (forced >= 0 && forced < k) return v[forced];
-    KInfo best = kernel_for(lg);
-    double best_cost = 0;
-    for (int i = 0; i < k; ++i) {
-        const int rc = resident_clusters(v[i], v[i].smem_for(J), s);
-        if (rc < 1) continue;
-        const double cost = (double)((nb + rc - 1) / rc) / v[i].cluster;
-        if (best_cost == 0 || cost < best_cost) best = v[i], best_cost = cost;
-    }
-    return best;
+    return k > 0 ? v[0] : kernel_for(lg);
 }
 int cf_kvariants_lg10(KInfo* out, int cap);
 int cf_kvariants_lg11(KInfo* out, int cap);
@@ -557,6 +552,23 @@ int cf_engine_set_max_ctas(cf_engine* e, int n) {
     return CF_OK;
 }
 
+long cf_resident_primes(cf_engine* e, int nmax, int Mmax, int J) {
+    if (!e || nmax < 1 || J < 0) return 0;
+    if (cudaSetDevice(e->device) != cudaSuccess) return 0;
+    std::vector<int> qn((size_t)std::max(J, 1), nmax), qM((size_t)std::max(J, 1), std::max(Mmax, nmax + 1));
+    Plan pl;
+    if (plan(e, nmax, 3, CF_MODEL_SUBSET, qn.data(), qM.data(), J, pl)) return 0;
+    const KInfo ki = pl.ki.cluster > 1 ? pick_cluster(e, pl.lg, 1, J, e->stream) : pl.ki;
+    const size_t smem = ki.smem_for(J);
+    if (ki.cluster > 1) return resident_clusters(ki, smem, e->stream);
+    int per_sm = 0, sms = 0;
+    if (cudaFuncSetAttribute((const void*)ki.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ki.fn, ki.threads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device) != cudaSuccess)
+        return 0;
+    return (long)per_sm * sms;
+}
+
 int cf_engine_set_transform_lg(cf_engine* e, int lg) {
     if (!e || lg < 0 || lg > MAX_LG_CLUSTER) return CF_ERR_ARG;
     e->min_lg = lg;
@@ -743,7 +755,7 @@ int cf_tune_variants(int lg, int* log2_entries, int* threads, int* ctas_per_sm, 
 
 int cf_tune_set(cf_engine* e, int lg, int variant) {
     if (e && lg > MAX_LG && lg <= MAX_LG_CLUSTER) {  // a cluster size, or -1: chosen per batch
-        KInfo v[4];
+        KInfo v[8];
         if (variant < -1 || variant >= cluster_variants(lg, v)) return CF_ERR_ARG;
         e->cluster_pick[lg - MAX_LG - 1] = variant;
         return CF_OK;
@@ -766,13 +778,15 @@ int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, i
     const u64 L = cfh::transform_length((u64)nmax);
     int lg = 0;
     while ((1ull << lg) < L) ++lg;
-    if (lg > MAX_LG) return fail(e, CF_ERR_UNSUPPORTED, "autotuning covers transforms up to 2^14; above, the cluster size follows the batch");
+    if (lg > MAX_LG_CLUSTER) return fail(e, CF_ERR_UNSUPPORTED, "transform length above 2^16");
+    const bool cl = lg > MAX_LG;  // cluster geometries: pinned through cluster_pick
     KInfo v[MAX_VARIANTS];
-    const int k = variants_for(lg, v, MAX_VARIANTS);
+    const int k = cl ? cluster_variants(lg, v) : variants_for(lg, v, MAX_VARIANTS);
+    int& pick = cl ? e->cluster_pick[lg - MAX_LG - 1] : e->tuned[lg];
     const std::vector<u64> primes = cfh::prime_range(0, B);
     const int qn[1] = {nmax}, qM[1] = {std::max(Mmax, nmax + 1)};
     std::vector<u64> first_out, out((size_t)B);
-    const int saved = e->tuned[lg];
+    const int saved = pick;
     int best = 0;
     double best_rate = -1;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -781,7 +795,7 @@ int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, i
     CF_CUDA(cudaEventCreate(&e1), "event");
     int rc = CF_OK;
     for (int i = 0; i < k && rc == CF_OK; ++i) {
-        e->tuned[lg] = i;
+        pick = i;
         float ms = 0;
         for (int rep = 0; rep < 2 && rc == CF_OK; ++rep) {  // a warm-up launch, then the timed one
             if (cudaEventRecord(e0, e->stream) != cudaSuccess) rc = fail(e, CF_ERR_CUDA, "event");
@@ -800,8 +814,8 @@ int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, i
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    e->tuned[lg] = rc == CF_OK ? best : saved;
-    if (chosen) *chosen = e->tuned[lg];
+    pick = rc == CF_OK ? best : saved;
+    if (chosen) *chosen = pick;
     return rc;
 }
 

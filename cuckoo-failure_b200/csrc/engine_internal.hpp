@@ -36,6 +36,8 @@ cfb::KInfo cf_kinfo_lg14_w();
 cfb::KInfo kernel_for(int lg, bool wide = false);
 cfb::KInfo cf_kinfo_lg15_c4();
 cfb::KInfo cf_kinfo_lg15_c8();
+cfb::KInfo cf_kinfo_lg15_c4_e8();
+cfb::KInfo cf_kinfo_lg15_c8_e8();
 cfb::KInfo cf_kinfo_lg16_c8();
 cfb::KInfo cf_kinfo_lg16_c16();
 constexpr int MAX_LG = 14;          // one CTA per prime (every entry point)

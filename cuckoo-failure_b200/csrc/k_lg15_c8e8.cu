@@ -1,0 +1,4 @@
+// Instantiation of the cluster kernel for transform length 2^15 on clusters of 8 CTAs, 8 entries per thread.
+#include "kernel_lg.cuh"
+
+cfb::KInfo cf_kinfo_lg15_c8_e8() { return cfb::kinfo_cluster<15, 3, 3>(); }

@@ -222,10 +222,11 @@ __global__ void __launch_bounds__(Geo<LG, R, LC>::CT, 1) k_suffix_cl(KParams kp)
     PrimeRun<G, DevExec<G>, false> pr(ex, kp, (int)blockIdx.x >> LC, smem);
     pr.run();
 }
-template <int LG, int LC>
+// 2^R entries per thread (16, or 8 for twice the threads per CTA when E = 8 >= C).
+template <int LG, int LC, int R = 4>
 inline KInfo kinfo_cluster() {
-    typedef Geo<LG, 4, LC> G;
-    return KInfo{&k_suffix_cl<LG, 4, LC>, G::CT, Smem<G>::BYTES, 4, nullptr, 1, G::C};
+    typedef Geo<LG, R, LC> G;
+    return KInfo{&k_suffix_cl<LG, R, LC>, G::CT, Smem<G>::BYTES, R, nullptr, 1, G::C};
 }
 // Another geometry of the 50-bit kernel (autotuning candidates): 2^R entries per thread, MB CTAs per SM.
 template <int LG, int R, int MB>

@@ -71,6 +71,8 @@ def lib():
         L.cf_engine_set_max_ctas.restype = ctypes.c_int
         L.cf_engine_set_transform_lg.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.cf_engine_set_transform_lg.restype = ctypes.c_int
+        L.cf_resident_primes.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.cf_resident_primes.restype = ctypes.c_long
         L.cf_tune_variants.argtypes = [ctypes.c_int, _intp, _intp, _intp, ctypes.c_int]
         L.cf_tune_variants.restype = ctypes.c_int
         L.cf_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -264,6 +266,10 @@ class Engine:
 
     def tune_get(self, lg):
         return int(lib().cf_tune_get(self._h, lg))
+
+    def resident_primes(self, nmax, Mmax, J=1):
+        """Primes one launch runs at the same time (SMs x CTAs per SM, or resident clusters)."""
+        return int(lib().cf_resident_primes(self._h, nmax, Mmax, J))
 
     def set_transform_lg(self, lg):
         """Transforms of at least 2^lg entries (0: the reference's length); residues do not change."""

@@ -93,6 +93,12 @@ uint64_t cf_workspace_bytes(int nmax, int Mmax, int J);
 /* Largest number of primes one launch can hold in the device's free memory (0 if none). */
 long cf_max_batch(cf_engine* e, int nmax, int Mmax, int J);
 
+/* Primes one launch runs at the same time for a table of nmax (J queries up to Mmax): the SMs times
+ * the CTAs per SM of the kernel, or for nmax > 16384 the thread-block clusters (one per prime)
+ * the device holds at once.  A batch that is a multiple of it runs in whole waves; 0 on error.
+ * No counterpart in the reference, whose batch is bounded by memory only (:743-780). */
+long cf_resident_primes(cf_engine* e, int nmax, int Mmax, int J);
+
 /* Kernel launches issued by the last cf_residues / cf_residues_async call. */
 long cf_last_launches(const cf_engine* e);
 
@@ -128,10 +134,10 @@ void cf_batch_graph_destroy(cf_batch_graph* g);
  * index).  cf_tune_set / cf_tune_get pin or read the choice (e.g. from a cache of earlier runs).
  * Primes below 2^62 always use the default geometry.
  * Transform lengths 2^15 and 2^16 (nmax > 16384) run one prime per thread-block cluster: their
- * variants are the cluster sizes compiled (smaller first; threads = CTA size, 16 entries each, one
- * CTA per SM).  By default a launch takes the size with the fewest waves of resident clusters per
- * CTA of a prime; cf_tune_set(e, lg, i) pins variant i, -1 goes back to that choice, and cf_tune_get
- * returns the pinned index or -1.  cf_autotune does not time them. */
+ * variants are the cluster geometries compiled (threads = CTA size, 2^log2_entries entries each,
+ * one CTA per SM; the cluster size is L / (threads 2^log2_entries)).  The default is the first,
+ * the fastest measured on B200; cf_tune_set(e, lg, i) pins variant i (-1: the default again),
+ * cf_tune_get returns the pinned index or -1, and cf_autotune times them like the others. */
 int cf_tune_variants(int lg, int* log2_entries, int* threads, int* ctas_per_sm, int cap);
 int cf_autotune(cf_engine* e, int nmax, int Mmax, int d, int B, double* rates, int cap, int* chosen);
 int cf_tune_set(cf_engine* e, int lg, int variant);

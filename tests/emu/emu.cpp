@@ -115,9 +115,9 @@ struct HostExec {
 };
 
 // The cluster kernel (transform length 2^LG on 2^LC CTAs per prime, 16 entries per thread).
-template <int LG, int LC>
+template <int LG, int LC, int R = 4>
 static int run_cluster(const KParams& kp) {
-    typedef Geo<LG, 4, LC> G;
+    typedef Geo<LG, R, LC> G;
     const size_t words = Smem<G>::bytes_for(kp.J) / 8;
     for (int b = 0; b < kp.B; ++b) {
         ClusterShared cs;
@@ -348,7 +348,8 @@ extern "C" int emu_residues_geo(const uint64_t* primes, int B, int nmax, int d, 
     return err ? -5 : 0;
 }
 // The cluster kernels on a table of any size (the transform length forced to 2^lg, as
-// cf_engine_set_transform_lg does): lg = 15 with C = 4 or 8, lg = 16 with C = 8 or 16.
+// cf_engine_set_transform_lg does): lg = 15 with C = 4 or 8 (-4, -8: 8 entries per thread instead
+// of 16), lg = 16 with C = 8 or 16.
 extern "C" int emu_residues_cluster(const uint64_t* primes, int B, int nmax, int d, int model, const int* qn,
                                     const int* qM, int J, uint64_t* out, int lg, int C) {
     int F = nmax;
@@ -363,7 +364,9 @@ extern "C" int emu_residues_cluster(const uint64_t* primes, int B, int nmax, int
     kp.model = model, kp.J = J, kp.qn = qn, kp.qM = qM, kp.ws = ws.data(), kp.ws_words = lo.total, kp.lay = lo;
     kp.out = out, kp.err = &err;
     try {
-        if (lg == 15 && C == 4) run_cluster<15, 2>(kp);
+        if (lg == 15 && C == -4) run_cluster<15, 2, 3>(kp);  // 8 entries per thread
+        else if (lg == 15 && C == -8) run_cluster<15, 3, 3>(kp);
+        else if (lg == 15 && C == 4) run_cluster<15, 2>(kp);
         else if (lg == 15 && C == 8) run_cluster<15, 3>(kp);
         else if (lg == 16 && C == 8) run_cluster<16, 3>(kp);
         else if (lg == 16 && C == 16) run_cluster<16, 4>(kp);

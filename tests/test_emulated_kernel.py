@@ -121,7 +121,7 @@ def emu_cluster(primes, nmax, d, queries, lg, C, model=0):
     return [[int(x) for x in out[b * J:(b + 1) * J]] for b in range(B)]
 
 
-@pytest.mark.parametrize("lg,C", [(15, 4), (15, 8), (16, 8), (16, 16)])
+@pytest.mark.parametrize("lg,C", [(15, 4), (15, 8), (15, -4), (15, -8), (16, 8), (16, 16)])  # -C: 8 entries per thread
 @pytest.mark.parametrize("model", [0, 1])
 def test_emulated_cluster_kernel_matches_oracle(lg, C, model):
     """Tables above n = 16384 run one prime per cluster of CTAs: pass 0 of each transform on every
@@ -132,4 +132,6 @@ def test_emulated_cluster_kernel_matches_oracle(lg, C, model):
     ps = h.oracle_primes(0, 2)
     # rows spread over two or three CTAs (512 or 256 threads each), so every cross-CTA path runs
     nmax, d, qs = (600, 3, [(600, 1500), (513, 1100), (5, 9)]) if model == 0 else (300, 2, [(300, 700), (17, 20)])
+    if C == -4:  # 1024 threads per CTA
+        nmax, qs = 1100, [(1100, 2500), (1030, 1100)] if model == 0 else [(1100, 2500), (17, 20)]
     assert emu_cluster(ps, nmax, d, qs, lg, C, model) == [h.oracle_residues(p, nmax, d, qs, model) for p in ps]

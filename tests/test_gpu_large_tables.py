@@ -16,12 +16,12 @@ pytestmark = pytest.mark.gpu
 CLI = os.path.join(h.ROOT, "cuckoo-failure_b200", "bin", "cuckoo_fast_b200")
 
 
-@pytest.mark.parametrize("lg,variant", [(15, 0), (15, 1), (16, 0), (16, 1)])
+@pytest.mark.parametrize("lg,variant", [(15, 0), (15, 1), (15, 2), (15, 3), (16, 0), (16, 1)])
 @pytest.mark.parametrize("model", [0, 1])
 def test_cluster_kernels_match_oracle_on_small_tables(lg, variant, model):
     ps = cb.prime_range(0, 3)
     # rows spread over two or three CTAs of the cluster (512 or 256 threads each)
-    nmax, d, qs = (700, 3, [(700, 1500), (513, 1100), (7, 9)]) if model == 0 else (300, 2, [(300, 700), (64, 65)])
+    nmax, d, qs = (1300, 3, [(1300, 2700), (1030, 2100), (513, 1100), (7, 9)]) if model == 0 else (1100, 2, [(1100, 2300), (64, 65)])
     with cb.Engine(0) as eng:
         eng.set_transform_lg(lg)
         eng.tune_set(lg, variant)
