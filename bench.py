@@ -594,30 +594,45 @@ def main():
         peak_gbs, which = hbm_peak()
         hbm = {"achieved": gbs, "peak": peak_gbs, "unit": "GB/s", "frac": gbs / peak_gbs, "peak_source": which}
     eng.close()  # its workspace (a wave of tables) goes back before the runs below allocate theirs
-    sweep = None
-    if rank == 0 and world == 1 and not a.no_sweep and n == 16384:
+
+    def section(fn, *args, **kw):
+        """A secondary measurement: its failure is reported in its own key, never in place of the
+        headline line."""
+        try:
+            return fn(*args, **kw)
+        except Exception as exc:  # noqa: BLE001 - recorded in the JSON line
+            print(f"bench: {fn.__name__} failed: {exc!r}", file=sys.stderr)
+            return {"error": repr(exc)[:300]}
+
+    solo = rank == 0 and world == 1
+
+    def sweep_fn():
         with cb.Engine(local) as eng2:
-            sweep = sweep_run(eng2, n, M, B)
-        for v in sweep.values():
+            out = sweep_run(eng2, n, M, B)
+        for v in out.values():
             v["frac"] = v["frac"] / peak if peak else None
-    cfg2 = None
-    if rank == 0 and world == 1 and not a.no_config2:
-        cfg2 = config2_run(local)
+        return out
+
+    def cfg2_fn():
+        out = config2_run(local)
         for k in ("default", "tuned"):
-            cfg2[k]["frac"] = cfg2[k].pop("frac_top") / peak if peak else None
-    large = None
-    if rank == 0 and world == 1 and not a.no_large:
-        large = large_run(local)
-    unev = None
-    if rank == 0 and world == 1 and not a.no_uneven:
+            out[k]["frac"] = out[k].pop("frac_top") / peak if peak else None
+        return out
+
+    def uneven_fn():
         with cb.Engine(local) as eng2:
-            unev = uneven_run(eng2, a.uneven_stride)
+            return uneven_run(eng2, a.uneven_stride)
+
+    sweep = section(sweep_fn) if solo and not a.no_sweep and n == 16384 else None
+    cfg2 = section(cfg2_fn) if solo and not a.no_config2 else None
+    large = section(large_run, local) if solo and not a.no_large else None
+    unev = section(uneven_fn) if solo and not a.no_uneven else None
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline and os.path.exists(reference_binary()[0]):
-        cpu = cpu_baseline(n, M, d)
+    if solo and not a.no_cpu_baseline and os.path.exists(reference_binary()[0]):
+        cpu = section(cpu_baseline, n, M, d)
     serving = None
-    if rank == 0 and world == 1 and not a.no_serving:
-        serving = serving_run(local, a.serve_seconds, full_seconds=a.serve_full_seconds)
+    if solo and not a.no_serving:
+        serving = section(serving_run, local, a.serve_seconds, full_seconds=a.serve_full_seconds)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,

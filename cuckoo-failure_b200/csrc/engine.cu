@@ -194,6 +194,11 @@ static int ensure_queries(cf_engine* e, const int* qn, const int* qM, int J, cud
 }
 
 static long fit_batch(size_t per_prime) {
+    // memory the stream-ordered pool keeps from freed resident tables counts as free: give it back
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+        cudaMemPoolTrimTo(pool, 0);
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return 0;
     const size_t reserve = (size_t)1 << 30;  // leave 1 GiB for the context, staging and other users

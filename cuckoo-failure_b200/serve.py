@@ -135,8 +135,16 @@ class GpuBackend:
     def free(tab):
         tab.close()
 
+    def _close_plain_engine(self):
+        e = getattr(self._plain_local, "eng", None)
+        if e is not None:
+            e.close()
+            self._plain_local.eng = None
+
     def close(self):
+        self.plain_pool.submit(self._close_plain_engine).result()  # the worker's engine, in its thread
         self.plain_pool.shutdown(wait=True)
+        self.torch.cuda.synchronize(self.device)  # tables freed in stream order are back in the pool
         self.eng.close()
 
 
