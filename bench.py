@@ -601,6 +601,9 @@ def main():
         try:
             return fn(*args, **kw)
         except Exception as exc:  # noqa: BLE001 - recorded in the JSON line
+            import traceback
+
+            traceback.print_exc()
             print(f"bench: {fn.__name__} failed: {exc!r}", file=sys.stderr)
             return {"error": repr(exc)[:300]}
 
