@@ -237,10 +237,13 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
     // chunk: as many primes as the workspace (grown once) holds
     long cap = (long)(e->ws_bytes / per_prime);
     if (fixed_ws && cap < 1) return fail(e, CF_ERR_NOMEM, "workspace holds no prime");
-    if (cap < B && !fixed_ws) {
+    // primes per launch this call wants: the batch, or at most max_ctas (whose workspace is then
+    // all it takes, so a capped engine leaves the rest of the device to others)
+    const long need = e->max_ctas > 0 ? std::min<long>(B, e->max_ctas) : B;
+    if (cap < need && !fixed_ws) {
         long fitb = fit_batch(per_prime) + cap;  // what is free plus what is already held
         if (fitb < 1) return fail(e, CF_ERR_NOMEM, "not enough device memory for one prime");
-        const long want = std::min<long>(B, fitb);
+        const long want = std::min<long>(need, fitb);
         int rc = ensure_ws(e, (size_t)want * per_prime);
         if (rc) return rc;
         cap = want;
