@@ -24,6 +24,9 @@ import tempfile
 import threading
 import time
 
+# the serving run overlaps streams (builds, queries, plain rebuilds): keep them on separate hardware
+# work queues; read when the CUDA context is created, so it is set before anything touches the GPU
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "cuckoo-failure_b200")
 sys.path.insert(0, PKG)
@@ -355,9 +358,9 @@ def config2_run(device, n=4096, M=8192, d=3, waves=4, reps=3):
 
 
 def sweep_run(eng, n, M, B, reps=2):
-    """Config-3 sweep at n = 16384, M = 2n: d = 2 and 4 (subset model) and the replacement model at
-    d = 3, one graph-captured 148-prime launch per step, the residues of primes 0 and 1 checked
-    where the reference has them."""
+    """Config-3 sweep at n = 16384, M = 2n: d = 2 and 4 (subset model), the replacement model at
+    d = 3, and d = 3 on the list of primes below 2^62 (the reference's -DFP_RB=64 build); one
+    graph-captured 148-prime launch per step, the residues checked where the reference has them."""
     import numpy as np
     import torch
 
@@ -365,8 +368,10 @@ def sweep_run(eng, n, M, B, reps=2):
 
     out = {}
     stream = torch.cuda.Stream()
-    for d, model in ((2, cb.MODEL_SUBSET), (4, cb.MODEL_SUBSET), (3, cb.MODEL_REPLACEMENT)):
-        primes = cb.prime_range(0, B)
+    for d, model, bits in ((2, cb.MODEL_SUBSET, 50), (4, cb.MODEL_SUBSET, 50), (3, cb.MODEL_REPLACEMENT, 50),
+                           (3, cb.MODEL_SUBSET, 62)):
+        primes = cb.prime_range(0, B, bits=bits)
+        assert cb.lib().cf_engine_set_prime_bits(eng._h, bits) == 0  # the graph does not read its primes
         d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
         d_out = torch.empty(B, dtype=torch.int64, device="cuda")
         g = eng.batch_graph(d_primes.data_ptr(), B, n, d, [(n, M)], d_out.data_ptr(), model=model)
@@ -375,12 +380,13 @@ def sweep_run(eng, n, M, B, reps=2):
         g.close()
         got = d_out.cpu().numpy().view(np.uint64)
         if model == cb.MODEL_SUBSET:
-            for i, r in golden_check(n, M, d).items():
-                assert int(got[i]) == r, f"d={d}: residue mismatch at prime {i}"
-        key = f"d{d}" + ("_replacement" if model else "")
+            for i, r in golden_check(n, M, d, bits).items():
+                assert int(got[i]) == r, f"d={d}, {bits}-bit primes: residue mismatch at prime {i}"
+        key = f"d{d}" + ("_replacement" if model else "") + ("_62bit" if bits == 62 else "")
         out[key] = {"value": B / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": reps,
-                    "primes_needed": cb.need(n, M, d, model),
+                    "primes_needed": cb.need(n, M, d, model, bits=bits),
                     "frac": B * algorithmic_mm(n) * K_OPS_PER_MM / (ms * 1e-3) / 1e12}
+    assert cb.lib().cf_engine_set_prime_bits(eng._h, 50) == 0
     return out
 
 

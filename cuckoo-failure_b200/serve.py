@@ -36,6 +36,12 @@ import os
 import sys
 import threading
 import time
+
+# Builds, queries and plain rebuilds run on separate streams.  With the driver's default of 8
+# hardware work queues, two streams can share one, and a query launched after a plain rebuild's
+# queued chunks would wait for all of them; 32 queues keep the streams apart.  It must be set
+# before the process creates its CUDA context.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 from collections import OrderedDict
 
 import numpy as np
@@ -127,9 +133,34 @@ class GpuBackend:
             self._plain_local.eng = e
         return e
 
+    def _plain_job(self, primes, n, M, d, model):
+        """The worker's rebuild of one request: primes in through pinned memory, the launches on the
+        worker's own stream, the residues back into pinned memory, and an event polled, so the worker
+        never sits inside a blocking CUDA call while the serving loop uses the device."""
+        torch = self.torch
+        eng = self._plain_engine()
+        st = getattr(self._plain_local, "stream", None)
+        if st is None:
+            st = self._plain_local.stream = torch.cuda.Stream(self.device)
+        dev = f"cuda:{self.device}"
+        B = len(primes)
+        host_p = torch.from_numpy(np.asarray(primes, dtype=np.uint64).view(np.int64)).pin_memory()
+        host_o = torch.empty(B, dtype=torch.int64, pin_memory=True)
+        with torch.cuda.stream(st):
+            d_p = host_p.to(dev, non_blocking=True)
+            d_o = torch.empty(B, dtype=torch.int64, device=dev)
+        eng.residues_async(d_p.data_ptr(), B, n, d, [(n, M)], d_o.data_ptr(), st.cuda_stream, model=model)
+        with torch.cuda.stream(st):
+            host_o.copy_(d_o, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(st)
+        while not ev.query():
+            time.sleep(0.002)
+        return host_o.numpy().view(np.uint64).copy()
+
     def plain(self, primes, n, M, d, model):
         """Future of the residues [prime] of (n, M) rebuilt alone, on the worker."""
-        return self.plain_pool.submit(lambda: self._plain_engine().residues(primes, n, d, [(n, M)], model=model)[:, 0])
+        return self.plain_pool.submit(self._plain_job, primes, n, M, d, model)
 
     @staticmethod
     def free(tab):
