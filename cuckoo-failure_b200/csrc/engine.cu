@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -387,8 +388,38 @@ struct cf_tables {
     int* d_err = nullptr;     // the build's device error word
     int* h_err = nullptr;     // its pinned host copy, written when the build is done
     cudaEvent_t built = nullptr;
-    bool pooled = false;      // keep / d_primes from the stream-ordered allocator
+    bool pooled = false;      // keep / d_primes / d_err from the stream-ordered allocator
+    bool err_slot = false;    // h_err is a slot of the shared pinned slab
 };
+
+// Pinned host words for the stream-ordered builds' error copies, taken from one slab allocated
+// once per process: freeing pinned memory (cudaFreeHost) waits for the whole device, which would
+// stall a serving loop that frees tables while rebuilds run.  Beyond the slab, plain pinned
+// allocations are used.
+namespace {
+constexpr int ERR_SLOTS = 4096;
+std::mutex g_slab_mu;
+int* g_slab = nullptr;
+std::vector<int> g_slab_free;
+int* take_err_slot() {
+    std::lock_guard<std::mutex> lk(g_slab_mu);
+    if (!g_slab) {
+        if (cudaHostAlloc(&g_slab, sizeof(int) * ERR_SLOTS, cudaHostAllocPortable) != cudaSuccess) {
+            g_slab = nullptr;
+            return nullptr;
+        }
+        for (int i = ERR_SLOTS - 1; i >= 0; --i) g_slab_free.push_back(i);
+    }
+    if (g_slab_free.empty()) return nullptr;
+    const int i = g_slab_free.back();
+    g_slab_free.pop_back();
+    return g_slab + i;
+}
+void give_err_slot(int* p) {
+    std::lock_guard<std::mutex> lk(g_slab_mu);
+    g_slab_free.push_back((int)(p - g_slab));
+}
+}  // namespace
 
 uint64_t cf_tables_bytes(int nmax, int Fmax) {
     if (nmax < 1) return 0;
@@ -421,8 +452,9 @@ static int tables_build(cf_engine* e, const uint64_t* primes, int B, int nmax, i
     const size_t kb = 8 * t->keep_words * (size_t)B;
     cudaError_t c = pooled ? cudaMallocAsync(&t->keep, kb, s) : cudaMalloc(&t->keep, kb);
     if (c == cudaSuccess) c = pooled ? cudaMallocAsync(&t->d_primes, 8 * (size_t)B, s) : cudaMalloc(&t->d_primes, 8 * (size_t)B);
-    if (c == cudaSuccess) c = cudaMalloc(&t->d_err, sizeof(int));
-    if (c == cudaSuccess) c = cudaHostAlloc(&t->h_err, sizeof(int), cudaHostAllocDefault);
+    if (c == cudaSuccess) c = pooled ? cudaMallocAsync(&t->d_err, sizeof(int), s) : cudaMalloc(&t->d_err, sizeof(int));
+    if (c == cudaSuccess && pooled && (t->h_err = take_err_slot()) != nullptr) t->err_slot = true;
+    if (c == cudaSuccess && !t->h_err) c = cudaHostAlloc(&t->h_err, sizeof(int), cudaHostAllocDefault);
     if (c == cudaSuccess) c = cudaEventCreateWithFlags(&t->built, cudaEventDisableTiming);
     if (c == cudaSuccess) c = cudaMemcpyAsync(t->d_primes, primes, 8 * (size_t)B, cudaMemcpyHostToDevice, s);
     if (c != cudaSuccess) {
@@ -543,13 +575,15 @@ void cf_tables_free(cf_tables* t) {
     if (t->pooled) {  // back to the pool in stream order, without waiting for the device
         cudaFreeAsync(t->keep, 0);
         cudaFreeAsync(t->d_primes, 0);
+        cudaFreeAsync(t->d_err, 0);
     } else {
         cudaFree(t->keep);
         cudaFree(t->d_primes);
+        cudaFree(t->d_err);
     }
-    cudaFree(t->d_out);
-    cudaFree(t->d_err);
-    if (t->h_err) cudaFreeHost(t->h_err);
+    cudaFree(t->d_out);  // only the waiting query form allocates it
+    if (t->err_slot) give_err_slot(t->h_err);
+    else if (t->h_err) cudaFreeHost(t->h_err);
     if (t->built) cudaEventDestroy(t->built);
     delete t;
 }
