@@ -9,7 +9,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
 EMU_SO = os.path.join(ROOT, "tests", "emu", "libcfemu.so")
-EMU_SRC = os.path.join(ROOT, "tests", "emu", "emu.cpp")
+EMU_DIR = os.path.join(ROOT, "tests", "emu")
+EMU_SRCS = [os.path.join(EMU_DIR, f) for f in ("emu.cpp", "emu_big.cpp", "emu_geo.cpp", "emu_cluster.cpp")]
 
 u64 = ctypes.c_uint64
 ci = ctypes.c_int
@@ -21,8 +22,16 @@ def build_test_libs():
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
     csrc = os.path.join(ROOT, "cuckoo-failure_b200", "csrc")
     newest = max(os.path.getmtime(os.path.join(csrc, f)) for f in os.listdir(csrc))
-    if not os.path.exists(EMU_SO) or os.path.getmtime(EMU_SO) < max(newest, os.path.getmtime(EMU_SRC)):
-        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", EMU_SRC, "-o", EMU_SO], check=True)
+    newest = max([newest, os.path.getmtime(os.path.join(EMU_DIR, "emu_exec.hpp"))] + [os.path.getmtime(f) for f in EMU_SRCS])
+    if not os.path.exists(EMU_SO) or os.path.getmtime(EMU_SO) < newest:
+        objs = [os.path.splitext(f)[0] + ".o" for f in EMU_SRCS]
+        procs = [subprocess.Popen(["g++", "-O2", "-std=c++17", "-fPIC", "-pthread", "-c", f, "-o", o])
+                 for f, o in zip(EMU_SRCS, objs)]  # the units compile in parallel
+        if any(p.wait() for p in procs):
+            raise RuntimeError("the emulation harness did not compile")
+        subprocess.run(["g++", "-shared", "-pthread"] + objs + ["-o", EMU_SO], check=True)
+        for o in objs:
+            os.remove(o)
 
 
 _oracle = None

@@ -59,3 +59,15 @@ def test_large_tables_refuse_what_they_do_not_cover():
             eng.residues(cb.prime_range(0, 1, bits=62), 20000, 3, [(20000, 40000)])
         with pytest.raises(cb.EngineError):  # beyond 2^16
             eng.residues(cb.prime_range(0, 1), 70000, 3, [(70000, 140000)])
+
+
+def test_resident_primes_gives_whole_waves():
+    import torch
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    with cb.Engine(0) as eng:
+        one = eng.resident_primes(16384, 32768)  # one CTA of 1024 threads per SM
+        cl4 = eng.resident_primes(32768, 65536)  # clusters of 4 CTAs, one per SM
+        cl8 = eng.resident_primes(65536, 131072)  # clusters of 8
+    assert one == sms
+    assert 0 < 4 * cl4 <= sms and 0 < 8 * cl8 <= sms
