@@ -81,9 +81,8 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "need queries with 8 <= max n < 2^%d\n", cfh::TWO_ADIC);
         return 2;
     }
-    if (cf_transform_length((uint64_t)nmax) > (bits == 62 ? 16384 : 65536)) {
-        std::fprintf(stderr, "this build handles tables up to n = %d with %d-bit primes (got %d)\n",
-                     bits == 62 ? 16384 : 65536, bits, nmax);
+    if (cf_transform_length((uint64_t)nmax) > 65536) {
+        std::fprintf(stderr, "this build handles tables up to n = 65536 (got %d)\n", nmax);
         return 2;
     }
 

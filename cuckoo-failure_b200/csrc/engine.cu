@@ -31,6 +31,8 @@ KInfo kernel_for(int lg, bool wide) {
             case 12: return cf_kinfo_lg12_w();
             case 13: return cf_kinfo_lg13_w();
             case 14: return cf_kinfo_lg14_w();
+            case 15: return cf_kinfo_lg15_c4_w();
+            case 16: return cf_kinfo_lg16_c8_w();
             default: return KInfo{nullptr, 0, 0, 0};
         }
     switch (lg) {
@@ -52,7 +54,12 @@ KInfo kernel_for(int lg, bool wide) {
 }
 // The cluster geometries compiled for transform length 2^lg (15, 16): cluster size, and 16 or 8
 // entries per thread (8: twice the threads per CTA); smaller clusters first.
-static int cluster_variants(int lg, KInfo* v) {
+static int cluster_variants(int lg, KInfo* v, bool wide = false) {
+    if (wide) {  // primes below 2^62: the default geometry only
+        if (lg != 15 && lg != 16) return 0;
+        v[0] = kernel_for(lg, true);
+        return 1;
+    }
     if (lg == 15)
         return v[0] = cf_kinfo_lg15_c4(), v[1] = cf_kinfo_lg15_c8(), v[2] = cf_kinfo_lg15_c4_e8(), v[3] = cf_kinfo_lg15_c8_e8(), 4;
     if (lg == 16) return v[0] = cf_kinfo_lg16_c8(), v[1] = cf_kinfo_lg16_c16(), 2;
@@ -76,9 +83,10 @@ static int resident_clusters(const KInfo& ki, size_t smem, cudaStream_t s) {
 }
 // The cluster geometry a launch at transform length 2^lg runs: the one pinned on the engine
 // (cf_tune_set, or cf_autotune's choice), else the default, the first of cluster_variants.
-static KInfo pick_cluster(const cf_engine* e, int lg, int nb, int J, cudaStream_t s) {
+static KInfo pick_cluster(const cf_engine* e, int lg, int nb, int J, cudaStream_t s, bool wide = false) {
     (void)nb, (void)J, (void)s;
     KInfo v[8];
+    if (wide) return kernel_for(lg, true);
     const int k = cluster_variants(lg, v);
     const int forced = lg > MAX_LG ? e->cluster_pick[lg - MAX_LG - 1] : -1;
     if (forced >= 0 && forced < k) return v[forced];
@@ -122,8 +130,6 @@ struct Plan {
 // The kernel this engine runs for the plan and the workspace layout its geometry needs (the
 // pass-0 twiddle tables follow the entries per thread); again whenever wide or F changes.
 static int finalize(cf_engine* e, Plan& pl) {
-    if (pl.wide && pl.lg > MAX_LG)
-        return fail(e, CF_ERR_UNSUPPORTED, "primes of 2^50 and above run with transforms up to 2^14 (nmax <= 16384)");
     pl.ki = kernel_of(e, pl.lg, pl.wide);
     if (!pl.ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     const int nw = pl.ki.threads >= 32 ? pl.ki.threads / 32 : 1;
@@ -228,7 +234,7 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
     KInfo ki = pl.ki;
     if (!ki.fn) return fail(e, CF_ERR_UNSUPPORTED, "no kernel for this transform length");
     if (ki.cluster > 1 && keep) return fail(e, CF_ERR_UNSUPPORTED, "resident tables are built up to nmax = 16384");
-    if (ki.cluster > 1) ki = pick_cluster(e, pl.lg, B, J, s);  // refined per chunk below
+    if (ki.cluster > 1) ki = pick_cluster(e, pl.lg, B, J, s, pl.wide);  // refined per chunk below
     size_t smem = ki.smem_for(J);
     int rc0 = check_smem(e, smem, J);
     if (rc0) return rc0;
@@ -274,7 +280,7 @@ static int launch_batch(cf_engine* e, const u64* d_primes, int B, int nmax, int 
         kp.keep = keep ? keep + (size_t)at * keep_words : nullptr;
         kp.keep_words = keep_words;
         if (ki.cluster > 1) {  // one cluster of ki.cluster CTAs per prime
-            ki = pick_cluster(e, pl.lg, nb, J, s);
+            ki = pick_cluster(e, pl.lg, nb, J, s, pl.wide);
             smem = ki.smem_for(J);
             rc0 = check_smem(e, smem, J);
             if (rc0) return rc0;

@@ -37,11 +37,13 @@ cfb::KInfo kernel_for(int lg, bool wide = false);
 cfb::KInfo cf_kinfo_lg15_c4();
 cfb::KInfo cf_kinfo_lg15_c8();
 cfb::KInfo cf_kinfo_lg15_c4_e8();
+cfb::KInfo cf_kinfo_lg15_c4_w();
+cfb::KInfo cf_kinfo_lg16_c8_w();
 cfb::KInfo cf_kinfo_lg15_c8_e8();
 cfb::KInfo cf_kinfo_lg16_c8();
 cfb::KInfo cf_kinfo_lg16_c16();
 constexpr int MAX_LG = 14;          // one CTA per prime (every entry point)
-constexpr int MAX_LG_CLUSTER = 16;  // a cluster of CTAs per prime (cf_residues and its forms, primes below 2^50)
+constexpr int MAX_LG_CLUSTER = 16;  // a cluster of CTAs per prime (cf_residues and its forms)
 constexpr int MAX_CLUSTER = 16;     // the largest cluster a layout provides row sums for
 struct cf_engine;
 // CF_OK if a launch with J queries fits the device's shared memory per block (engine.cu)

@@ -214,19 +214,20 @@ inline KInfo kinfo() {
 }
 // Transform lengths above 2^14 (tables above n = 16384, primes below 2^50): one prime per cluster of
 // 2^LC CTAs, one CTA per SM, launched with that cluster size (CTA b 2^LC + c is CTA c of prime b).
-template <int LG, int R, int LC>
+template <int LG, int R, int LC, bool W>
 __global__ void __launch_bounds__(Geo<LG, R, LC>::CT, 1) k_suffix_cl(KParams kp) {
     typedef Geo<LG, R, LC> G;
     extern __shared__ __align__(16) u64 smem[];
     DevExec<G> ex;
-    PrimeRun<G, DevExec<G>, false> pr(ex, kp, (int)blockIdx.x >> LC, smem);
+    PrimeRun<G, DevExec<G>, W> pr(ex, kp, (int)blockIdx.x >> LC, smem);
     pr.run();
 }
-// 2^R entries per thread (16, or 8 for twice the threads per CTA when E = 8 >= C).
-template <int LG, int LC, int R = 4>
+// 2^R entries per thread (16, or 8 for twice the threads per CTA when E = 8 >= C); W: primes
+// below 2^62 (otherwise below 2^50).
+template <int LG, int LC, int R = 4, bool W = false>
 inline KInfo kinfo_cluster() {
     typedef Geo<LG, R, LC> G;
-    return KInfo{&k_suffix_cl<LG, R, LC>, G::CT, Smem<G>::BYTES, R, nullptr, 1, G::C};
+    return KInfo{&k_suffix_cl<LG, R, LC, W>, G::CT, Smem<G>::BYTES, R, nullptr, 1, G::C};
 }
 // Another geometry of the 50-bit kernel (autotuning candidates): 2^R entries per thread, MB CTAs per SM.
 template <int LG, int R, int MB>

@@ -399,7 +399,6 @@ struct PrimeRun {
     static constexpr int C = G::C, CT = G::CT, LCN = G::LCN;  // a cluster of C CTAs of CT threads per prime
     static constexpr bool CG = C > 1;  // loads of what other CTAs wrote go to L2 (ldp / lds / ldc)
     static_assert(W || G::LG <= 14 || G::FRED, "reduction-free forward transform needs 2^LG p < 2^64");
-    static_assert(!W || C == 1, "primes below 2^62 run on one CTA per prime");
     static_assert(NP > 1, "layout 0 must hold index t + jT in slot j of thread t");
     // L = 2^14 (1024 threads x 16 entries): the kernel spectrum lives in tensor memory, each
     // thread's 16 (value, companion) pairs in its own 64 columns (all 512 columns of the SM's 128

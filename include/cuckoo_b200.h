@@ -72,8 +72,7 @@ const char* cf_engine_last_error(const cf_engine* e);
  * Replaces the body of the batch loop, fast/cuckoo_fast.cu:787-901: per-prime tables (:797-839),
  * the step loop (:841-855), k_query (:867-876) and the Horner finish (:877-890).
  * Requirements: 1 <= qn[j] <= nmax <= 65536, qM[j] > qn[j], d <= qM[j] for the subset model, every
- * prime odd, < 2^62 (< 2^50 when nmax > 16384), > max(nmax, qM), with transform_length(nmax)
- * dividing p - 1.  Tables up to nmax = 16384 take one CTA per prime; larger ones a thread-block
+ * prime odd, < 2^62, > max(nmax, qM), with transform_length(nmax) dividing p - 1.  Tables up to nmax = 16384 take one CTA per prime; larger ones a thread-block
  * cluster of 4 to 16 CTAs per prime (the reference runs up to nmax < 2^20, :61, :692, with all of
  * a GPU's threads on a batch of primes).
  * Host buffers; returns when the residues are in `residues`. */

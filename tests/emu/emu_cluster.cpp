@@ -20,8 +20,13 @@ extern "C" int emu_residues_cluster(const uint64_t* primes, int B, int nmax, int
     kp.primes = primes, kp.B = B, kp.n = nmax, kp.F = F, kp.d = d, kp.d0 = model == MODEL_SUBSET ? d : 1;
     kp.model = model, kp.J = J, kp.qn = qn, kp.qM = qM, kp.ws = ws.data(), kp.ws_words = lo.total, kp.lay = lo;
     kp.out = out, kp.err = &err;
+    bool wide = false;  // primes below 2^62: the engine's cluster kernels for them
+    for (int b = 0; b < B; ++b) wide = wide || primes[b] >= (1ull << 50);
     try {
-        if (lg == 15 && C == -4) run_cluster<15, 2, 3>(kp);  // 8 entries per thread
+        if (wide && lg == 15 && C == 4) run_cluster<15, 2, 4, true>(kp);
+        else if (wide && lg == 16 && C == 8) run_cluster<16, 3, 4, true>(kp);
+        else if (wide) return -4;
+        else if (lg == 15 && C == -4) run_cluster<15, 2, 3>(kp);  // 8 entries per thread
         else if (lg == 15 && C == -8) run_cluster<15, 3, 3>(kp);
         else if (lg == 15 && C == 4) run_cluster<15, 2>(kp);
         else if (lg == 15 && C == 8) run_cluster<15, 3>(kp);

@@ -116,7 +116,7 @@ struct HostExec {
 };
 
 // The cluster kernel (transform length 2^LG on 2^LC CTAs per prime, 16 entries per thread).
-template <int LG, int LC, int R = 4>
+template <int LG, int LC, int R = 4, bool W = false>
 inline int run_cluster(const KParams& kp) {
     typedef Geo<LG, R, LC> G;
     const size_t words = Smem<G>::bytes_for(kp.J) / 8;
@@ -133,7 +133,7 @@ inline int run_cluster(const KParams& kp) {
                 try {
                     HostExec<G> ex;
                     ex.rk = c, ex.cl = &cs, ex.own = sm[c].data();
-                    PrimeRun<G, HostExec<G>, false> pr(ex, kp, b, sm[c].data());
+                    PrimeRun<G, HostExec<G>, W> pr(ex, kp, b, sm[c].data());
                     pr.run();
                 } catch (const std::exception& e) {
                     errs[c] = e.what();

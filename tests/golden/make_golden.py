@@ -12,8 +12,9 @@ Run from the repository root, where the reference tree is available:
 Groups: `base` (small sizes, config 2, one or two primes at n = 16384, the library CLI at small n),
 `large` (the replacement model at n = 4096 and 16384 through the library's --mod P, 18 queries
 at n <= 16384, and a seeded sample of the uneven-batch workload) and `huge` (tables above
-n = 16384: n = 32768 and n = 65536, primes 0 and 1, one host-build process per prime; the
-n = 65536 runs take 32 GB of host memory each and run one after the other).
+n = 16384: n = 32768 and n = 65536, primes 0 and 1, one host-build process per prime, and
+n = 32768 with 62-bit primes; the n = 65536 runs take 32 GB of host memory each and run one after
+the other).
 """
 import argparse
 import concurrent.futures as cf
@@ -139,6 +140,14 @@ def huge():
             g.write(f"# d=3 queries={' '.join(f'{a},{b}' for a, b in queries)} first=0 count=2 (one run per prime)\n")
             g.write("".join(outs))
         print(name, sum(len(o.splitlines()) for o in outs), "lines")
+    # 62-bit primes (-DFP_RB=64) at n = 32768, primes 0 and 1
+    b64 = os.path.join(REF, "cuckoo_fast_cpu64")
+    q = [(32768, 65536), (20000, 50000)]
+    with cf.ThreadPoolExecutor(2) as ex:
+        outs = list(ex.map(lambda i: fast_lines(3, q, i, 1, binary=b64), (0, 1)))
+    with open(os.path.join(HERE, "fast62_n32768_d3.txt"), "w") as g:
+        g.write(f"# d=3 queries={' '.join(f'{a},{b}' for a, b in q)} first=0 count=2 (one run per prime)\n")
+        g.write("".join(outs))
 
 
 def main():

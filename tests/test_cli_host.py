@@ -17,8 +17,6 @@ def test_cli_usage_and_bad_queries(tmp_path):
     assert run(["3", str(q), "0", "5"]).returncode == 2  # max n below 8
     q.write_text("70000 140000\n")
     assert run(["3", str(q), "0", "5"]).returncode == 2  # beyond this build's table size
-    q.write_text("20000 40000\n")
-    assert run(["3", str(q), "0", "5", "--prime-bits", "62"]).returncode == 2  # 62-bit primes stop at 16384
     assert run(["3", str(tmp_path / "missing.txt"), "0", "5"]).returncode == 2
     q.write_text("100 200\n")
     assert run(["3", str(q), "0", "5", "--bogus"]).returncode == 2

@@ -135,3 +135,14 @@ def test_emulated_cluster_kernel_matches_oracle(lg, C, model):
     if C == -4:  # 1024 threads per CTA
         nmax, qs = 1100, [(1100, 2500), (1030, 1100)] if model == 0 else [(1100, 2500), (17, 20)]
     assert emu_cluster(ps, nmax, d, qs, lg, C, model) == [h.oracle_residues(p, nmax, d, qs, model) for p in ps]
+
+
+@pytest.mark.parametrize("lg,C", [(15, 4), (16, 8)])
+def test_emulated_cluster_kernel_62bit_primes(lg, C):
+    """The cluster kernels for primes below 2^62 (transforms kept in [0, 2p)), at the top of the
+    reference's -DFP_RB=64 list, rows over two CTAs."""
+    import cuckoo_b200 as cb
+
+    ps = cb.prime_range(0, 2, bits=62)
+    nmax, d, qs = 600, 3, [(600, 1500), (513, 1100)]
+    assert emu_cluster(ps, nmax, d, qs, lg, C) == [h.oracle_residues(p, nmax, d, qs) for p in ps]

@@ -31,7 +31,7 @@ def test_cluster_kernels_match_oracle_on_small_tables(lg, variant, model):
         assert [int(x) for x in row] == h.oracle_residues(p, nmax, d, qs, model), (lg, variant, p)
 
 
-@pytest.mark.parametrize("name", ["fast_n32768_d3.txt", "fast_n65536_d3.txt"])
+@pytest.mark.parametrize("name", ["fast_n32768_d3.txt", "fast_n65536_d3.txt", "fast62_n32768_d3.txt"])
 def test_large_tables_match_reference(name):
     d, queries, first, count, lines = h.load_fast_golden(name)
     exp = h.expected_by_prime(lines)
@@ -55,10 +55,21 @@ def test_cli_at_n32768_prints_the_reference_lines():
 
 def test_large_tables_refuse_what_they_do_not_cover():
     with cb.Engine(0) as eng:
-        with pytest.raises(cb.EngineError):  # 62-bit primes stop at transform length 2^14
-            eng.residues(cb.prime_range(0, 1, bits=62), 20000, 3, [(20000, 40000)])
         with pytest.raises(cb.EngineError):  # beyond 2^16
             eng.residues(cb.prime_range(0, 1), 70000, 3, [(70000, 140000)])
+        with pytest.raises(cb.EngineError):  # resident tables stop at 16384
+            eng.tables(cb.prime_range(0, 1), 20000, 40000, 3)
+
+
+@pytest.mark.parametrize("lg", [15, 16])
+def test_62bit_cluster_kernels_match_oracle_on_small_tables(lg):
+    ps = cb.prime_range(0, 2, bits=62)
+    nmax, d, qs = 700, 3, [(700, 1500), (513, 1100), (7, 9)]
+    with cb.Engine(0) as eng:
+        eng.set_transform_lg(lg)
+        got = eng.residues(ps, nmax, d, qs)
+    for p, row in zip(ps, got):
+        assert [int(x) for x in row] == h.oracle_residues(p, nmax, d, qs), (lg, p)
 
 
 def test_resident_primes_gives_whole_waves():
