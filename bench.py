@@ -425,6 +425,30 @@ def large_run(device, sizes=((32768, 65536), (65536, 131072)), d=3, reps=1):
         out[f"n{n}"] = {"value": B / (ms * 1e-3), "unit": UNIT, "primes_per_launch": B, "ms_per_launch": ms,
                         "one_prime_alone_s": one * 1e-3, "workload": f"n={n}, M={M}, d={d}, one query, 50-bit primes",
                         "checked": "residues of primes 0 and 1 equal the reference host build's"}
+    # the reference's published case: n = 65536 with 126 queries (the seeded set of the fixture)
+    path = os.path.join(ROOT, "tests", "golden", "fast_n65536_d3_J126.txt")
+    if os.path.exists(path):
+        with open(path) as f:
+            head = f.readline()
+            want = {(int(t[2]), int(t[3])): int(t[4]) for t in (ln.split() for ln in f) if len(t) == 5 and t[0] == "0"}
+        qs = [tuple(int(x) for x in tok.split(",")) for tok in head.split("queries=")[1].split(" first=")[0].split()]
+        n, M = 65536, max(m for _, m in qs)
+        with cb.Engine(device) as eng:
+            fit, wave = max(1, eng.max_batch(n, M, len(qs)) - 1), eng.resident_primes(n, M, len(qs))
+            B = fit - fit % wave if wave and fit > wave else fit
+            primes = cb.prime_range(0, B)
+            d_primes = torch.tensor(np.array(primes, dtype=np.uint64).view(np.int64), device="cuda")
+            d_out = torch.empty(B * len(qs), dtype=torch.int64, device="cuda")
+            g = eng.batch_graph(d_primes.data_ptr(), B, n, d, qs, d_out.data_ptr())
+            ms = timed_replays(g.launch, stream, reps)
+            g.status(stream.cuda_stream)
+            g.close()
+            got = d_out.cpu().numpy().view(np.uint64)[:len(qs)]
+            assert all(int(r) == want[q] for q, r in zip(qs, got)), "n=65536, 126 queries: residue mismatch at prime 0"
+        out["n65536_J126"] = {"value": B / (ms * 1e-3), "unit": UNIT, "primes_per_launch": B, "ms_per_launch": ms,
+                              "queries": len(qs), "s_per_prime_at_this_rate": ms * 1e-3 / B,
+                              "workload": "n=65536, d=3, 126 queries (n from 2000 to 65536, M = n U[1.5, 4], seeded)",
+                              "checked": "all 126 residues of prime 0 equal the reference host build's"}
     out["reference_published"] = ("fast/README.md:80-86: n = 65536, one prime, 126 queries, CUDA batch 2 on an H100: "
                                   "table build 3.5 s per prime, queries 0.75 s (current version)")
     return out

@@ -140,6 +140,16 @@ def huge():
             g.write(f"# d=3 queries={' '.join(f'{a},{b}' for a, b in queries)} first=0 count=2 (one run per prime)\n")
             g.write("".join(outs))
         print(name, sum(len(o.splitlines()) for o in outs), "lines")
+    # the reference's published case at n = 65536 has 126 queries (fast/README.md:80-86): a seeded
+    # set of 126 (n, M), n log-uniform in [2000, 65536] with 65536 itself, M = n U[1.5, 4]; prime 0
+    import numpy as np
+
+    rng = np.random.default_rng(126)
+    ns = [65536] + sorted({int(x) for x in np.exp(rng.uniform(np.log(2000), np.log(65536), 140))}, reverse=True)
+    q126 = [(n, int(round(n * rng.uniform(1.5, 4.0)))) for n in ns[:126]]
+    with open(os.path.join(HERE, "fast_n65536_d3_J126.txt"), "w") as g:
+        g.write(f"# d=3 queries={' '.join(f'{a},{b}' for a, b in q126)} first=0 count=1\n")
+        g.write(fast_lines(3, q126, 0, 1))
     # 62-bit primes (-DFP_RB=64) at n = 32768, primes 0 and 1
     b64 = os.path.join(REF, "cuckoo_fast_cpu64")
     q = [(32768, 65536), (20000, 50000)]

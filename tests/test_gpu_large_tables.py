@@ -31,7 +31,8 @@ def test_cluster_kernels_match_oracle_on_small_tables(lg, variant, model):
         assert [int(x) for x in row] == h.oracle_residues(p, nmax, d, qs, model), (lg, variant, p)
 
 
-@pytest.mark.parametrize("name", ["fast_n32768_d3.txt", "fast_n65536_d3.txt", "fast62_n32768_d3.txt"])
+@pytest.mark.parametrize("name", ["fast_n32768_d3.txt", "fast_n65536_d3.txt", "fast62_n32768_d3.txt",
+                                  "fast_n65536_d3_J126.txt"])
 def test_large_tables_match_reference(name):
     d, queries, first, count, lines = h.load_fast_golden(name)
     exp = h.expected_by_prime(lines)
