@@ -17,8 +17,8 @@ EXACT = [r for r in h.load_lib_golden() if r[0] == "exact"]
 
 
 def test_prime_set_of_config_1():
-    """Survey measurement of the reference: 152 primes for n=200, M=400, d=3, from 4276092929 down
-    to 104857601; 169 with --replacement."""
+    """What the reference's library CLI prints for n=200, M=400, d=3: 152 primes, from 4276092929
+    down to 104857601; 169 with --replacement."""
     ps = cb.lib_primes(200, 400, 3)
     assert len(ps) == 152 and ps[0] == 4276092929 and ps[-1] == 104857601
     assert ps == sorted(ps, reverse=True) and len(set(ps)) == len(ps)
