@@ -1080,17 +1080,42 @@ struct PrimeRun {
             ex.each([&](int t, Regs<G>& rg) CF_INL {
                 const u64* iv = inv() + 2 * (size_t)Mj;  // the pair of 1/(M_j - w) sits at iv - 2w
                 const int tw = t & ~31;                  // the warp's first thread
-                u64 acc = 0, c0 = 0, q0 = 0;
-                if (G::idx(0, t, 0) < q) ldp<CG>(iv - 2 * G::idx(0, t, 0), c0, q0);
+                u64 acc = 0;
+                if constexpr (C == 1) {  // the next slot's inverse loaded one slot ahead
+                    u64 c0 = 0, q0 = 0;
+                    if (G::idx(0, t, 0) < q) ldp<CG>(iv - 2 * G::idx(0, t, 0), c0, q0);
 #pragma unroll
-                for (int j = 0; j < E; ++j) {
-                    const bool more = j + 1 < E && G::idx(0, tw, j + 1) < q;
-                    u64 c1 = 0, q1 = 0;  // slots at or above q multiply by zero
-                    if (more && G::idx(0, t, j + 1) < q) ldp<CG>(iv - 2 * G::idx(0, t, j + 1), c1, q1);
-                    if constexpr (W) acc = madd(acc, canon(shoup_mul_lazy(rg.x[j], c0, q0, P)), P);
-                    else acc += shoup_mul_lazy(rg.x[j], c0, q0, P);  // E terms below 4p: < 2^57
-                    if (!more) break;
-                    c0 = c1, q0 = q1;
+                    for (int j = 0; j < E; ++j) {
+                        const bool more = j + 1 < E && G::idx(0, tw, j + 1) < q;
+                        u64 c1 = 0, q1 = 0;  // slots at or above q multiply by zero
+                        if (more && G::idx(0, t, j + 1) < q) ldp<CG>(iv - 2 * G::idx(0, t, j + 1), c1, q1);
+                        if constexpr (W) acc = madd(acc, canon(shoup_mul_lazy(rg.x[j], c0, q0, P)), P);
+                        else acc += shoup_mul_lazy(rg.x[j], c0, q0, P);  // E terms below 4p: < 2^57
+                        if (!more) break;
+                        c0 = c1, q0 = q1;
+                    }
+                } else {
+                    // A cluster's CTAs have half the warps of the 2^14 kernel to hide the inverses'
+                    // L2 latency: they load QD slots ahead (a ring of QD + 1 pairs).  Measured at
+                    // n = 65536 with 126 queries: 8.29 against 8.86 s per launch; with one query the
+                    // deeper ring cost the 2^14 kernel 1.5 %, so that kernel keeps one slot.
+                    constexpr int QD = 4;
+                    u64 rc[QD + 1], rq[QD + 1];
+#pragma unroll
+                    for (int j = 0; j < QD + 1; ++j) rc[j] = rq[j] = 0;
+#pragma unroll
+                    for (int j = 0; j < QD && j < E; ++j)
+                        if (G::idx(0, t, j) < q) ldp<CG>(iv - 2 * G::idx(0, t, j), rc[j], rq[j]);
+#pragma unroll
+                    for (int j = 0; j < E; ++j) {
+                        if (G::idx(0, tw, j) >= q) break;  // warp-uniform: this slot and the later ones lie past the row
+                        const int jn = j + QD;
+                        if (jn < E && G::idx(0, t, jn) < q) ldp<CG>(iv - 2 * G::idx(0, t, jn), rc[jn % (QD + 1)], rq[jn % (QD + 1)]);
+                        const u64 c0 = G::idx(0, t, j) < q ? rc[j % (QD + 1)] : 0;  // slots at or above q multiply by zero
+                        const u64 q0 = G::idx(0, t, j) < q ? rq[j % (QD + 1)] : 0;
+                        if constexpr (W) acc = madd(acc, canon(shoup_mul_lazy(rg.x[j], c0, q0, P)), P);
+                        else acc += shoup_mul_lazy(rg.x[j], c0, q0, P);  // E terms below 4p: < 2^57
+                    }
                 }
                 const u64 part = canon(shoup_mul_lazy(acc, 1, misc()[MI_ONEQ], P));
                 ex.warp_sum_store(lt(t), part, P, qs + (size_t)jq * NW, 1);
