@@ -174,9 +174,9 @@ int cf_tables_build_async(cf_engine* e, const uint64_t* primes, int B, int nmax,
 int cf_tables_ready(const cf_tables* t);
 int cf_tables_query_async(cf_engine* e, const cf_tables* t, const int* qn, const int* qM, int J, uint64_t* d_residues,
                           void* stream);
-/* At most n primes (CTAs) per launch for this engine's batches (0: no cap), so a long batch leaves
- * SMs to work on other streams; the engine's workspace then holds at most n primes, so it leaves
- * the rest of the device memory to others too. */
+/* At most n primes per launch for this engine's batches (0: no cap): n CTAs up to nmax = 16384,
+ * n clusters above.  A long batch then leaves SMs to work on other streams, and the engine's
+ * workspace holds at most n primes, leaving the rest of the device memory to others too. */
 int cf_engine_set_max_ctas(cf_engine* e, int n);
 
 /* Transforms of at least 2^lg entries for this engine's batches (0, the default: the reference's
